@@ -1,0 +1,569 @@
+"""Benchmark of the DoseCUDA B200 dose engines.
+
+Headline: CCCS ms/beam on the small photon workload (128^3 voxels at 2.5 mm,
+water with a lung block and a bone cube, one 10x10 cm 6 MV field, 100 MU,
+72 cone directions).  One step = one control point: density -> ray trace ->
+TERMA -> collapsed-cone dose.  Secondary (same JSON line): IMPT spots/s on the
+small proton workload (96^3 at 2 mm, 6 energy layers x 100 spots); one step =
+one beam: RLSP -> WET ray trace + smoothing -> pencil-beam dose.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl mine|reference]
+
+``value`` is measured with the inputs resident in HBM (CUDA events on the
+launching stream, L2 flushed between steps with a 256 MiB write outside the
+timed brackets); ``e2e`` goes through the drop-in ``dose_kernels`` API with
+host buffers (pinned input, H2D + D2H inside the timed region).
+``--impl reference`` times the reference DoseCUDA CUDA extension (built from
+the reference sources into oracle/_ref/) through its own API on the same
+inputs.  N > 1 (torchrun): N independent replicas, one per GPU, no
+collective on the data path (weak scaling); times are the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import glob
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+PEAKS_FALLBACK = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
+SM_COUNT = 148
+FP32_LANES_PER_SM = 128
+
+
+# ----------------------------------------------------------------------------
+# multi-process plumbing
+# ----------------------------------------------------------------------------
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def init_dist(ws, backend):
+    if ws <= 1:
+        return None
+    import datetime
+    import torch.distributed as dist
+    dist.init_process_group(backend=backend, timeout=datetime.timedelta(seconds=120))
+    return dist
+
+
+def aggregate_max(value: float, dist_mod) -> float:
+    """Max of a per-rank scalar over all ranks (identity without a group)."""
+    if dist_mod is None:
+        return value
+    import torch
+    dev = "cuda" if dist_mod.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([value], dtype=torch.float64, device=dev)
+    dist_mod.all_reduce(t, op=dist_mod.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(dist_mod):
+    if dist_mod is not None:
+        dist_mod.barrier()
+
+
+# ----------------------------------------------------------------------------
+# clocks
+# ----------------------------------------------------------------------------
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.Q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self._t = threading.Thread(target=self._read, daemon=True)
+            self._t.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            p = [x.strip() for x in ln.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                mx = float(p[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, p[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ----------------------------------------------------------------------------
+# workloads
+# ----------------------------------------------------------------------------
+def photon_workload():
+    from dosecuda_b200 import phantoms
+    grid, plan = phantoms.photon_small()
+    model = plan.beam_models[0]
+    cp = plan.beam_list[0].cp_list[0]
+    density = grid.DensityFromHU(plan.machine_name)
+    return grid, model, cp, density
+
+
+def proton_workload():
+    from dosecuda_b200 import phantoms
+    grid, plan = phantoms.proton_small()
+    model = plan.beam_models[0]
+    beam = plan.beam_list[0]
+    rlsp = grid.RLSPFromHU(plan.machine_name)
+    return grid, model, beam, rlsp
+
+
+def load_oracle():
+    """The CPU oracle module (oracle/oracle.py), loaded by path: it is the
+    checker and the CPU baseline, never part of the measured engine."""
+    import importlib.util
+    if "dc_oracle" in sys.modules:
+        return sys.modules["dc_oracle"]
+    spec = importlib.util.spec_from_file_location("dc_oracle", os.path.join(ROOT, "oracle", "oracle.py"))
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules["dc_oracle"] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            p = json.load(f)
+        return p, "measured"
+    return PEAKS_FALLBACK, "fallback"
+
+
+# ----------------------------------------------------------------------------
+# algorithmic work (counted on the host from geometry, independent of the kernels)
+# ----------------------------------------------------------------------------
+def cccs_samples(dose_ref_mask_count: int, model, spacing_mm: float) -> int:
+    """Cone samples per active voxel: 12 azimuths x sum over cones of the
+    float sample count of the backward march (ray_length, -= spacing)."""
+    per = 0
+    sp = np.float32(spacing_mm) / np.float32(10.0)
+    for rl in np.asarray(model.kernel, np.float32)[:, 5]:
+        r = np.float32(rl)
+        while r >= 0:
+            per += 1
+            r = np.float32(r - sp)
+    return 12 * per * dose_ref_mask_count
+
+
+# ----------------------------------------------------------------------------
+def time_steps(step, k, flush):
+    """Device time of k steps (CUDA events on the current stream around each
+    step; the L2 flush between steps is outside the brackets)."""
+    import torch
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(k)]
+    for i in range(k):
+        flush()
+        ev[i][0].record()
+        step()
+        ev[i][1].record()
+    torch.cuda.synchronize()
+    return sum(a.elapsed_time(b) for a, b in ev)
+
+
+def run_mine(args, ws, rank, local, dist_mod):
+    import torch
+    from dosecuda_b200 import _lib, dose_kernels, engine
+    from dosecuda_b200.dose_kernels import ControlPointView, PhotonModelView
+    from dosecuda_b200.plan import VolumeObject
+
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    lib = _lib.load()
+    flush_buf = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+
+    def flush():
+        flush_buf.zero_()
+
+    pk, pk_kind = peaks()
+    out = {}
+
+    # ---------------- photon (headline) ----------------
+    grid, model, cp, density = photon_workload()
+    dens_t = torch.from_numpy(density).to(dev)
+    dose_t = torch.empty_like(dens_t)
+    views = (PhotonModelView(model), ControlPointView(cp))
+
+    def step_x():
+        engine.photon_dose(dens_t, grid, model, cp, out=dose_t, views=views)
+
+    for _ in range(args.warmup):
+        flush()
+        step_x()
+    torch.cuda.synchronize()
+    barrier(dist_mod)
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        t_ms = time_steps(step_x, args.steps, flush)
+    torch.cuda.synchronize()
+    barrier(dist_mod)
+    t_ms = aggregate_max(t_ms, dist_mod)
+    x_ms_per_beam = t_ms / (args.steps * ws)
+
+    # kernel-level timing on the launching stream (profiled pass, separate from the timed one)
+    _lib.raise_for(lib.dc_profile_enable(local, 1))
+    _lib.raise_for(lib.dc_profile_reset(local))
+    for _ in range(args.steps):
+        flush()
+        step_x()
+    torch.cuda.synchronize()
+    prof_x = _lib.profile_read(local)
+    _lib.raise_for(lib.dc_profile_enable(local, 0))
+    dose_np = dose_t.cpu().numpy()
+    # active voxels = TERMA > 0.01 (the voxels the CCCS evaluates); from the
+    # engine's TERMA mask we only need the count, taken as dose > 0 voxels.
+    n_active = int((dose_np > 0).sum())
+    samples = cccs_samples(n_active, model, float(grid.spacing[0]))
+    c_launches, c_ms = prof_x.get("cccs", (1, float("nan")))
+    cccs_avg_ms = c_ms / max(c_launches, 1)
+    flops_per_sample = 18.0
+    fp32_peak = SM_COUNT * FP32_LANES_PER_SM * 2 * pk.get("sm_max_mhz", 1965.0) * 1e6 / 1e12
+    achieved_tf = samples * flops_per_sample / (cccs_avg_ms * 1e-3) / 1e12
+    nvox = density.size
+    cccs_bytes = nvox * 4 * 2 + n_active * 4  # electron + dose + TERMA mask read (algorithmic)
+
+    # e2e through the drop-in API (pinned host input, H2D + D2H per call)
+    pinned = torch.from_numpy(density).pin_memory()
+    vol = VolumeObject()
+    vol.voxel_data = pinned.numpy()
+    vol.origin = np.array(grid.origin, dtype=np.single)
+    vol.spacing = np.array(grid.spacing, dtype=np.single)
+    for _ in range(max(1, args.warmup)):
+        dose_kernels.photon_dose_cuda(model, vol, cp, local)
+    torch.cuda.synchronize()
+    barrier(dist_mod)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        d = dose_kernels.photon_dose_cuda(model, vol, cp, local)
+    torch.cuda.synchronize()
+    e2e_ms = (time.perf_counter() - t0) * 1e3
+    barrier(dist_mod)
+    e2e_ms = aggregate_max(e2e_ms, dist_mod)
+    parity_e2e = float(np.abs(d - dose_np).max())
+
+    # ---------------- proton (secondary) ----------------
+    pgrid, pmodel, pbeam, rlsp = proton_workload()
+    rl_t = torch.from_numpy(rlsp).to(dev)
+    wet_t = torch.empty_like(rl_t)
+    pdose_t = torch.empty_like(rl_t)
+    dmodel = engine.ProtonModelDevice(pmodel, device=dev)
+    n_spots = pbeam.spot_list.shape[0]
+
+    def step_p():
+        engine.proton_wet(rl_t, pgrid, pbeam, pmodel, out=wet_t)
+        engine.proton_dose(wet_t, pgrid, pbeam, dmodel, out=pdose_t)
+
+    for _ in range(args.warmup):
+        flush()
+        step_p()
+    torch.cuda.synchronize()
+    barrier(dist_mod)
+    tp_ms = time_steps(step_p, args.steps, flush)
+    barrier(dist_mod)
+    tp_ms = aggregate_max(tp_ms, dist_mod)
+    spots_per_s = n_spots * args.steps * ws / (tp_ms * 1e-3)
+    _lib.raise_for(lib.dc_profile_enable(local, 1))
+    _lib.raise_for(lib.dc_profile_reset(local))
+    for _ in range(args.steps):
+        flush()
+        step_p()
+    torch.cuda.synchronize()
+    prof_p = _lib.profile_read(local)
+    _lib.raise_for(lib.dc_profile_enable(local, 0))
+    # (voxel, spot) pairs the pencil beam evaluates: voxels inside each layer's range
+    wet_np = wet_t.cpu().numpy() * np.float32(10.0)
+    pairs = 0
+    for e in np.unique(pbeam.spot_list[:, 3].astype(int)):
+        r80 = pmodel.divergence_params[e, 1]
+        pairs += int((wet_np <= np.float32(1.1) * r80).sum()) * int((pbeam.spot_list[:, 3].astype(int) == e).sum())
+    pb_launches, pb_ms = prof_p.get("pencil_beam", (1, float("nan")))
+    pb_avg_ms = pb_ms / max(pb_launches, 1)
+    pb_flops = pairs * 20.0
+    pvol = VolumeObject()
+    pvol.voxel_data = torch.from_numpy(rlsp).pin_memory().numpy()
+    pvol.origin = np.array(pgrid.origin, dtype=np.single)
+    pvol.spacing = np.array(pgrid.spacing, dtype=np.single)
+    for _ in range(max(1, args.warmup)):
+        w = dose_kernels.proton_raytrace_cuda(pmodel, pvol, pbeam, local)
+        wv = VolumeObject()
+        wv.voxel_data, wv.origin, wv.spacing = w, pvol.origin, pvol.spacing
+        dose_kernels.proton_spot_cuda(pmodel, pvol, wv, pbeam, local)
+    barrier(dist_mod)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        w = dose_kernels.proton_raytrace_cuda(pmodel, pvol, pbeam, local)
+        wv = VolumeObject()
+        wv.voxel_data, wv.origin, wv.spacing = w, pvol.origin, pvol.spacing
+        dose_kernels.proton_spot_cuda(pmodel, pvol, wv, pbeam, local)
+    pe2e_ms = (time.perf_counter() - t0) * 1e3
+    barrier(dist_mod)
+    pe2e_ms = aggregate_max(pe2e_ms, dist_mod)
+
+    out.update(dict(
+        x_ms_per_beam=x_ms_per_beam, t_ms=t_ms, prof_x=prof_x, clocks=clk.summary(), samples=samples,
+        n_active=n_active, cccs_avg_ms=cccs_avg_ms, achieved_tf=achieved_tf, fp32_peak=fp32_peak,
+        cccs_bytes=cccs_bytes, e2e_ms=e2e_ms, parity_e2e=parity_e2e, nvox=nvox, pk=pk, pk_kind=pk_kind,
+        spots_per_s=spots_per_s, tp_ms=tp_ms, prof_p=prof_p, pairs=pairs, pb_avg_ms=pb_avg_ms, pb_flops=pb_flops,
+        pe2e_ms=pe2e_ms, n_spots=n_spots, pnvox=rlsp.size,
+    ))
+    return out
+
+
+def cpu_baseline_photon():
+    """The FP64 C oracle on the host cores: one full control point of the
+    photon workload (the whole 128^3 beam; about 10-30 s of CPU time).
+    Also returns the oracle's CCCS sample count (voxels with TERMA > 0.01)."""
+    oracle = load_oracle()
+    grid, model, cp, density = photon_workload()
+    t0 = time.perf_counter()
+    _, _, _, samples = oracle.photon_dose(density, np.asarray(grid.spacing, np.float32)[[0, 0, 0]], grid.origin,
+                                          model, cp.iso, cp.mu, cp.ga, cp.ca, cp.ta, np.ascontiguousarray(cp.mlc),
+                                          intermediates=True)
+    dt = time.perf_counter() - t0
+    return {"value": round(dt * 1e3, 1), "unit": "ms/beam", "cores": oracle.num_threads(), "kind": "port",
+            "sample": "one full control point of the 128^3 photon workload (FP64 C/OpenMP oracle)"}, samples
+
+
+def cpu_baseline_proton():
+    oracle = load_oracle()
+    grid, model, beam, rlsp = proton_workload()
+    sp = np.asarray(grid.spacing, np.float32)[[0, 0, 0]]
+    t0 = time.perf_counter()
+    wet, _ = oracle.proton_wet(rlsp, sp, grid.origin, beam.iso, beam.gantry_angle, beam.couch_angle, model.VSADX,
+                               model.VSADY)
+    oracle.proton_dose(wet.astype(np.float32), sp, grid.origin, beam.iso, beam.gantry_angle, beam.couch_angle,
+                       model, beam.spot_list)
+    dt = time.perf_counter() - t0
+    return {"value": round(beam.spot_list.shape[0] / dt, 2), "unit": "spots/s", "cores": oracle.num_threads(),
+            "kind": "port",
+            "sample": "one full beam of the 96^3 proton workload (600 spots, FP64 C/OpenMP oracle)"}
+
+
+def main_mine(args):
+    import torch
+    ws, rank, local = dist_env()
+    dist_mod = init_dist(ws, "nccl" if torch.cuda.is_available() else "gloo")
+    r = run_mine(args, ws, rank, local, dist_mod)
+    if rank == 0:
+        cpu_x = cpu_p = None
+        if ws == 1 and not args.no_cpu:
+            cpu_x, oracle_samples = cpu_baseline_photon()
+            cpu_p = cpu_baseline_proton()
+            # algorithmic work counted by the oracle (TERMA > 0.01 voxels x cone samples)
+            r["achieved_tf"] *= oracle_samples / max(r["samples"], 1)
+            r["samples"] = oracle_samples
+        pk = r["pk"]
+        hbm = pk.get("hbm_gbs", PEAKS_FALLBACK["hbm_gbs"])
+        x_launch_per_step = 4  # wet_march, terma, cone_dirs, cccs
+        p_launch_per_step = 3  # wet_march, wet_smooth, pencil_beam
+        line = {
+            "metric": "CCCS ms/beam",
+            "value": round(r["x_ms_per_beam"], 4),
+            "unit": "ms/beam",
+            "n_gpus": ws,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": round(r["t_ms"] / args.steps, 4),
+            "higher_is_better": False,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f32",
+            "data": "synthetic (seeded phantoms; beam-model tables shipped with the reference)",
+            "config": {"workload": "photon CCCS small: 128^3 @ 2.5 mm, water + lung block + bone cube, 6 MV "
+                                   "10x10 cm MLC field, 100 MU, gantry 0, 72 cone directions",
+                       "step": "one control point: ray trace + TERMA + CCCS, density resident in HBM",
+                       "l2": "flushed between steps (256 MiB write, outside the timed brackets)",
+                       "parallelism": "replicas" if ws > 1 else "single GPU"},
+            "e2e": {"value": round(r["e2e_ms"] / (args.steps * ws), 4), "unit": "ms/beam",
+                    "h2d_bytes_per_step": int(r["nvox"] * 4), "d2h_bytes_per_step": int(r["nvox"] * 4),
+                    "api": "dosecuda_b200.dose_kernels.photon_dose_cuda (host numpy in/out, pinned input)"},
+            "roofline": {
+                "bound": "fp32",
+                "kernel": "cccs",
+                "achieved": round(r["achieved_tf"], 3),
+                "peak": round(r["fp32_peak"], 2),
+                "unit": "TFLOP/s",
+                "frac": round(r["achieved_tf"] / r["fp32_peak"], 4),
+                "peak_kind": "nominal FP32 (148 SMs x 128 lanes x 2 x max SM clock); no measured FP32 peak exists",
+                "work": f"{r['samples']} cone samples x 18 FP32 flops (+2 trilinear texture fetches, 1 SFU exp each)",
+                "samples_per_s": round(r["samples"] / (r["cccs_avg_ms"] * 1e-3), 1),
+                "kernel_ms": round(r["cccs_avg_ms"], 4),
+                "hbm": {"achieved_gbs": round(r["cccs_bytes"] / (r["cccs_avg_ms"] * 1e-3) / 1e9, 2),
+                        "peak_gbs": hbm, "frac": round(r["cccs_bytes"] / (r["cccs_avg_ms"] * 1e-3) / 1e9 / hbm, 5),
+                        "peak_kind": r["pk_kind"]},
+                "traffic": None,
+            },
+            "kernels": {k: {"launches": v[0], "total_ms": round(v[1], 4)} for k, v in r["prof_x"].items()},
+            "gpu_launches": x_launch_per_step * args.steps,
+            "clocks": r["clocks"],
+            "cpu_baseline": cpu_x,
+            "secondary": {
+                "metric": "IMPT spots/s",
+                "value": round(r["spots_per_s"], 1),
+                "unit": "spots/s",
+                "higher_is_better": True,
+                "ms_per_step": round(r["tp_ms"] / args.steps, 4),
+                "config": {"workload": "proton PB small: 96^3 @ 2 mm, water + bone cylinder + lung slab, gantry 0, "
+                                       "6 layers (energy ids 34..59) x 100 spots",
+                           "step": "one beam: WET ray trace + smoothing + pencil-beam dose, RLSP resident in HBM"},
+                "e2e": {"value": round(r["n_spots"] * args.steps * ws / (r["pe2e_ms"] * 1e-3), 1), "unit": "spots/s",
+                        "h2d_bytes_per_step": int(r["pnvox"] * 4 * 2), "d2h_bytes_per_step": int(r["pnvox"] * 4 * 2),
+                        "api": "dose_kernels.proton_raytrace_cuda + proton_spot_cuda (host numpy)"},
+                "roofline": {"bound": "fp32", "kernel": "pencil_beam",
+                             "achieved": round(r["pb_flops"] / (r["pb_avg_ms"] * 1e-3) / 1e12, 3),
+                             "peak": round(r["fp32_peak"], 2), "unit": "TFLOP/s",
+                             "frac": round(r["pb_flops"] / (r["pb_avg_ms"] * 1e-3) / 1e12 / r["fp32_peak"], 4),
+                             "work": f"{r['pairs']} (voxel, spot) pairs x 20 FP32 flops (+2 SFU exp each)",
+                             "pairs_per_s": round(r["pairs"] / (r["pb_avg_ms"] * 1e-3), 1),
+                             "kernel_ms": round(r["pb_avg_ms"], 4), "traffic": None},
+                "kernels": {k: {"launches": v[0], "total_ms": round(v[1], 4)} for k, v in r["prof_p"].items()},
+                "gpu_launches": p_launch_per_step * args.steps,
+                "cpu_baseline": cpu_p,
+            },
+        }
+        print(json.dumps(line))
+    if dist_mod is not None:
+        dist_mod.destroy_process_group()
+
+
+# ----------------------------------------------------------------------------
+def main_reference(args):
+    """The reference DoseCUDA CUDA extension through its own API, same inputs."""
+    ws, rank, local = dist_env()
+    if rank != 0:
+        return
+    ref_dir = os.path.join(ROOT, "oracle", "_ref")
+    if not glob.glob(os.path.join(ref_dir, "dose_kernels*.so")):
+        print(json.dumps({"impl": "reference", "unavailable": "reference build oracle/_ref missing "
+                                                               "(oracle/build_ref.sh needs the reference sources)"}))
+        return
+    sys.path.insert(0, ref_dir)
+    import dose_kernels as ref  # the reference build
+    from dosecuda_b200.plan import VolumeObject
+
+    grid, model, cp, density = photon_workload()
+    vol = VolumeObject()
+    vol.voxel_data = np.ascontiguousarray(density)
+    vol.origin = np.array(grid.origin, dtype=np.single)
+    vol.spacing = np.array(grid.spacing, dtype=np.single)
+    for _ in range(args.warmup):
+        ref.photon_dose_cuda(model, vol, cp, local)
+    with ClockSampler(local) as clk:
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            ref.photon_dose_cuda(model, vol, cp, local)
+        x_ms = (time.perf_counter() - t0) * 1e3 / args.steps
+
+    pgrid, pmodel, pbeam, rlsp = proton_workload()
+    pvol = VolumeObject()
+    pvol.voxel_data = np.ascontiguousarray(rlsp)
+    pvol.origin = np.array(pgrid.origin, dtype=np.single)
+    pvol.spacing = np.array(pgrid.spacing, dtype=np.single)
+
+    def beam_step():
+        w = ref.proton_raytrace_cuda(pmodel, pvol, pbeam, local)
+        wv = VolumeObject()
+        wv.voxel_data, wv.origin, wv.spacing = w, pvol.origin, pvol.spacing
+        ref.proton_spot_cuda(pmodel, pvol, wv, pbeam, local)
+
+    for _ in range(args.warmup):
+        beam_step()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        beam_step()
+    p_s = (time.perf_counter() - t0) / args.steps
+    n_spots = pbeam.spot_list.shape[0]
+    line = {
+        "impl": "reference",
+        "metric": "CCCS ms/beam",
+        "value": round(x_ms, 4),
+        "unit": "ms/beam",
+        "n_gpus": 1,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": round(x_ms, 4),
+        "higher_is_better": False,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic (seeded phantoms; beam-model tables shipped with the reference)",
+        "config": {"workload": "photon CCCS small: 128^3 @ 2.5 mm, water + lung block + bone cube, 6 MV "
+                               "10x10 cm MLC field, 100 MU, gantry 0, 72 cone directions",
+                   "step": "one control point through the reference's dose_kernels.photon_dose_cuda",
+                   "parallelism": "single GPU"},
+        "e2e": {"value": round(x_ms, 4), "unit": "ms/beam", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "cpu_baseline": {"value": round(x_ms, 4), "unit": "ms/beam", "cores": 1, "kind": "reference",
+                         "sample": "the reference's own implementation is CUDA-only: its extension built from the "
+                                   "reference sources for sm_100a, run on the B200 through its Python API with "
+                                   "host numpy buffers (its per-call allocation and copies included)"},
+        "clocks": clk.summary(),
+        "secondary": {"metric": "IMPT spots/s", "value": round(n_spots / p_s, 1), "unit": "spots/s",
+                      "higher_is_better": True, "ms_per_step": round(p_s * 1e3, 4),
+                      "e2e": {"value": round(n_spots / p_s, 1), "unit": "spots/s"}},
+    }
+    print(json.dumps(line))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="mine", choices=["mine", "reference"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU oracle baseline")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        main_reference(args)
+    else:
+        main_mine(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,43 @@
+// dc_photon.cuh — per-control-point parameter blocks of the photon engine.
+// Both are passed to the kernels by value (kernel-parameter constant bank), so
+// concurrent calls on different streams never share mutable device state.
+#pragma once
+
+#include "../../include/dosecuda.h"
+#include "dc_common.cuh"
+#include "dc_runtime.cuh"
+
+namespace dc {
+
+constexpr int kMaxPairs = 128;      // MLC leaf pairs
+constexpr int kMaxProfile = 64;     // off-axis profile points
+constexpr int kMaxSpectrum = 32;    // spectral energy bins
+constexpr int kMaxCones = 8;        // zenith cones (kernel.csv rows)
+constexpr int kMaxConeSteps = 512;  // summed samples per azimuth over all cones
+
+struct PhotonParams {
+    float psd, ssd, pss, sss, mlc_distance, ssw, ea, esw, efd;
+    int n_pairs, n_prof, n_spec;
+    float mlc_xl[kMaxPairs], mlc_xr[kMaxPairs], mlc_yb[kMaxPairs], mlc_yt[kMaxPairs];
+    float prof_r[kMaxProfile], prof_i[kMaxProfile], prof_s[kMaxProfile];
+    float spec_mu[kMaxSpectrum], spec_pw[kMaxSpectrum], spec_sw[kMaxSpectrum];
+};
+
+struct CccsCones {
+    int n_cones, total_steps;
+    float theta_deg[kMaxCones], Am[kMaxCones], am[kMaxCones], Bm[kMaxCones], bm[kMaxCones];
+    int step_off[kMaxCones], n_steps[kMaxCones];
+    float rl10[kMaxConeSteps];  // sample distance along the cone axis, mm
+};
+
+// Validates the model/control point and fills the parameter blocks.
+// spacing_cm is the CCCS step (the isotropic voxel spacing in cm).
+void build_photon_params(const dc_photon_model &m, const dc_control_point &cp, float spacing_cm,
+                         PhotonParams &P, CccsCones &C);
+
+// Enqueues ray trace -> TERMA -> CCCS for one control point on stream s.
+// The density volume must already be in ctx.density; dose_dev: device output.
+void run_photon_pipeline(DeviceContext &ctx, const Grid &g, const Frame &f, const PhotonParams &P,
+                         const CccsCones &C, float dose_scale, float *dose_dev, cudaStream_t s);
+
+}  // namespace dc

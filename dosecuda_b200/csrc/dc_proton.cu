@@ -1,0 +1,271 @@
+// dc_proton.cu — double-Gaussian proton pencil-beam dose.
+//
+// Restates pencilBeamKernel (IMPTClasses.cu:204-271) and its helpers
+// (interpolateProtonLUT :69-92, sigmaAir :94-102, nuclearHalo :104-121,
+// caxDistance :123-133).  For a voxel with smoothed WET w (mm) and an energy
+// layer with range R80, skipped when w > 1.1*R80:
+//   idd, sigma_mcs  = linear interpolation of the layer's LUT at depth w
+//   sigma_air       = A d^2 + B d + C,  d = |voxel - source| - w + 0.7 R80
+//   sigma_t         = sigma_air + sigma_mcs
+//   sigma_h, w_h    = empirical nuclear halo (function of w, R80)
+//   sigma_ht        = hypot(sigma_t, sigma_h)
+//   D += sum_spots MU * [ (1-w_h) idd/(2 pi sigma_t^2)  exp(-r^2/2 sigma_t^2)
+//                        +   w_h  idd/(2 pi sigma_ht^2) exp(-r^2/2 sigma_ht^2) ]
+// with r^2 the squared distance from the voxel (BEV coordinates) to the
+// spot's divergent axis.
+//
+// B200 mapping (instead of one thread per (voxel, layer) with a global
+// atomicAdd per pair of the reference): a CTA owns a 32x16 tile of voxels in
+// one z-slice, two voxels per thread, and walks all energy layers.  Per layer
+// the CTA stages the layer's LUT rows and spot records in shared memory
+// (broadcast reads in the spot loop); each thread keeps its voxels' dose in
+// registers across layers and writes each voxel once — no atomics, so the
+// result is deterministic.  The spot loop is two exponentials per
+// (voxel, spot) pair on the special-function unit (ex2.approx with the
+// log2(e) factor folded into the per-voxel Gaussian scales) plus ~12 FP32
+// operations, so the kernel is bound by the SFU issue rate.
+#include <algorithm>
+#include <cmath>
+#include <string>
+#include <vector>
+
+#include "../../include/dosecuda.h"
+#include "dc_common.cuh"
+#include "dc_kernels.cuh"
+#include "dc_runtime.cuh"
+
+namespace dc {
+
+constexpr int kPbThreadsX = 32;
+constexpr int kPbThreadsY = 8;
+constexpr int kPbVoxY = 2;      // voxels per thread along y
+constexpr int kPbSpotChunk = 512;
+
+void build_proton_tables(const float *spots, int n_spots, const float *dvp, int n_energies, int dvp_len,
+                         float vsadx, float vsady, std::vector<LayerRec> &layers,
+                         std::vector<SpotRec> &spot_recs) {
+    if (n_spots <= 0) throw Error(DC_ERR_VALUE, "'spot_list' must hold at least one spot.");
+    if (n_energies <= 0) throw Error(DC_ERR_VALUE, "'divergence_params' must hold at least one energy.");
+    if (dvp_len < 5) throw Error(DC_ERR_VALUE, "'divergence_params' rows must hold energy, R80, A, B, C.");
+    struct Tmp {
+        int e;
+        int order;
+        float x, y, mu;
+    };
+    std::vector<Tmp> tmp((size_t)n_spots);
+    for (int s = 0; s < n_spots; ++s) {
+        const float *r = spots + 4 * (size_t)s;
+        // static_cast<int> truncation of the energy column (dosemodule.cu:220).
+        const float ef = r[3];
+        if (!(ef > -1.0f) || !(ef < (float)n_energies)) {
+            throw Error(DC_ERR_VALUE, "spot " + std::to_string(s) + ": energy id " + std::to_string(ef) +
+                                          " outside the beam model's " + std::to_string(n_energies) +
+                                          " energies.");
+        }
+        tmp[s] = {static_cast<int>(ef), s, r[0], r[1], r[2]};
+    }
+    // Sort by energy id (dosemodule.cu:224); stable, so the summation order is
+    // reproducible.
+    std::stable_sort(tmp.begin(), tmp.end(), [](const Tmp &a, const Tmp &b) { return a.e < b.e; });
+    spot_recs.resize((size_t)n_spots);
+    for (int s = 0; s < n_spots; ++s) {
+        SpotRec &o = spot_recs[s];
+        o.x = tmp[s].x;
+        o.y = tmp[s].y;
+        o.mu = tmp[s].mu;
+        o.tx = tmp[s].x / vsadx;
+        o.ty = tmp[s].y / vsady;
+        o.inv_t2 = 1.0f / (o.tx * o.tx + o.ty * o.ty + 1.0f);
+        o.pad0 = o.pad1 = 0.f;
+    }
+    layers.clear();
+    int s = 0;
+    while (s < n_spots) {
+        int e = tmp[s].e;
+        int t = s;
+        while (t < n_spots && tmp[t].e == e) ++t;
+        LayerRec L;
+        L.spot_start = s;
+        L.n_spots = t - s;
+        L.energy_id = e;
+        const float *row = dvp + (size_t)dvp_len * e;
+        L.r80 = row[1];
+        L.A = row[2];
+        L.B = row[3];
+        L.C = row[4];
+        L.pad = 0.f;
+        layers.push_back(L);
+        s = t;
+    }
+}
+
+// Per (voxel, layer) Gaussian parameters.  Returns false if the layer does
+// not reach the voxel (w > 1.1 R80).
+struct PbVoxel {
+    float pf, hf;      // primary / halo amplitude (idd/(2 pi sigma^2) weighted)
+    float ps2, hs2;    // -0.5/sigma^2 * log2(e)
+};
+
+__device__ __forceinline__ bool pb_voxel_layer(const LayerRec &L, const float *s_depth, const float *s_sigma,
+                                               const float *s_idd, int lut_len, float wet_mm,
+                                               float dist_src, PbVoxel &o) {
+    const float r80 = L.r80;
+    if (wet_mm > 1.1f * r80) return false;
+    // interpolateProtonLUT (IMPTClasses.cu:69-92)
+    const int i = lower_bound(s_depth, lut_len, wet_mm);
+    float idd, sig;
+    if (i == lut_len) {
+        idd = s_idd[i - 1];
+        sig = s_sigma[i - 1];
+    } else if (i == 0) {
+        idd = s_idd[0];
+        sig = s_sigma[0];
+    } else {
+        const float fac = (wet_mm - s_depth[i - 1]) / (s_depth[i] - s_depth[i - 1]);
+        idd = fmaf(s_idd[i] - s_idd[i - 1], fac, s_idd[i - 1]);
+        sig = fmaf(s_sigma[i] - s_sigma[i - 1], fac, s_sigma[i - 1]);
+    }
+    // sigmaAir (IMPTClasses.cu:94-102)
+    const float d = dist_src - wet_mm + (0.7f * r80);
+    const float sigma_t = fmaf(fmaf(L.A, d, L.B), d, L.C) + sig;
+    // nuclearHalo (IMPTClasses.cu:104-121)
+    const float w = clampf(wet_mm, 0.1f, r80 - 0.1f);
+    const float hs_ = 2.85f + (0.0014f * r80 * logf(w + 3.0f)) + (0.06f * w) - (7.4e-5f * sqr(w)) -
+                      ((0.22f * r80) / sqr(w - r80 - 5.0f));
+    const float hw_ = 0.052f * logf(1.13f + (w / (11.2f - (0.023f * r80)))) +
+                      (0.35f * ((0.0017f * sqr(r80)) - r80) / (sqr(r80 + 3.0f) - sqr(w))) -
+                      (1.61e-9f * w * sqr(r80 + 3.0f));
+    const float sigma_h = fmaxf(hs_, 0.0f);
+    const float wh = clampf(hw_, 0.0f, 0.9f);
+    const float sigma_ht = hypotf(sigma_t, sigma_h);
+    o.pf = (1.0f - wh) * idd / (2.0f * CUDART_PI_F * sqr(sigma_t));
+    o.hf = wh * idd / (2.0f * CUDART_PI_F * sqr(sigma_ht));
+    o.ps2 = (sigma_t != 0.0f ? -0.5f / sqr(sigma_t) : -INFINITY) * kLog2e;
+    o.hs2 = (sigma_ht != 0.0f ? -0.5f / sqr(sigma_ht) : -INFINITY) * kLog2e;
+    return true;
+}
+
+__global__ void __launch_bounds__(kPbThreadsX *kPbThreadsY)
+    pencil_beam_kernel(Grid g, Frame f, ProtonTables t, const float *__restrict__ wet_s, float *__restrict__ dose) {
+    extern __shared__ float4 smem4[];
+    float4 *s_spot_a = smem4;                    // x, y, mu, -
+    float4 *s_spot_b = smem4 + kPbSpotChunk;     // tx, ty, inv_t2, -
+    float *s_lut = reinterpret_cast<float *>(smem4 + 2 * kPbSpotChunk);
+    float *s_depth = s_lut;
+    float *s_sigma = s_lut + t.lut_len;
+    float *s_idd = s_lut + 2 * t.lut_len;
+
+    const int tid = threadIdx.y * kPbThreadsX + threadIdx.x;
+    const int nthreads = kPbThreadsX * kPbThreadsY;
+    const int i = blockIdx.x * kPbThreadsX + threadIdx.x;
+    const int j0 = blockIdx.y * (kPbThreadsY * kPbVoxY) + threadIdx.y;
+    const int k = blockIdx.z;
+
+    float hx[kPbVoxY], hy[kPbVoxY], hz[kPbVoxY], hz2[kPbVoxY], wet_mm[kPbVoxY], dsrc[kPbVoxY], acc[kPbVoxY];
+    bool inside[kPbVoxY];
+#pragma unroll
+    for (int v = 0; v < kPbVoxY; ++v) {
+        const int j = j0 + v * kPbThreadsY;
+        inside[v] = (i < g.nx) && (j < g.ny);
+        acc[v] = 0.0f;
+        const int ic = min(i, g.nx - 1), jc = min(j, g.ny - 1);
+        const float3 p = voxel_xyz(g, f, ic, jc, k);
+        const float3 h = image_to_head<false>(f, p);
+        hx[v] = h.x;
+        hy[v] = h.y;
+        hz[v] = h.z;
+        hz2[v] = h.z * h.z;
+        dsrc[v] = distance_to_source(f, p);
+        wet_mm[v] = __ldg(wet_s + (long long)ic + (long long)g.nx * (jc + (long long)g.ny * k)) * 10.0f;
+    }
+
+    for (int l = 0; l < t.n_layers; ++l) {
+        const LayerRec L = t.layers[l];
+        __syncthreads();  // previous layer's shared data no longer in use
+        const float *gd = t.lut_depths + (size_t)L.energy_id * t.lut_len;
+        const float *gs = t.lut_sigmas + (size_t)L.energy_id * t.lut_len;
+        const float *gi = t.lut_idds + (size_t)L.energy_id * t.lut_len;
+        for (int q = tid; q < t.lut_len; q += nthreads) {
+            s_depth[q] = __ldg(gd + q);
+            s_sigma[q] = __ldg(gs + q);
+            s_idd[q] = __ldg(gi + q);
+        }
+        __syncthreads();
+
+        PbVoxel pv[kPbVoxY];
+        bool act[kPbVoxY];
+        bool any = false;
+#pragma unroll
+        for (int v = 0; v < kPbVoxY; ++v) {
+            act[v] = inside[v] && pb_voxel_layer(L, s_depth, s_sigma, s_idd, t.lut_len, wet_mm[v], dsrc[v], pv[v]);
+            if (!act[v]) {
+                pv[v].pf = pv[v].hf = 0.f;
+                pv[v].ps2 = pv[v].hs2 = 0.f;
+            }
+            any |= act[v];
+        }
+        const bool block_any = __syncthreads_or(any);
+        if (!block_any) continue;
+
+        for (int c0 = 0; c0 < L.n_spots; c0 += kPbSpotChunk) {
+            const int cn = min(kPbSpotChunk, L.n_spots - c0);
+            if (c0 > 0) __syncthreads();
+            const float4 *gsp = reinterpret_cast<const float4 *>(t.spots + L.spot_start + c0);
+            for (int q = tid; q < cn; q += nthreads) {
+                s_spot_a[q] = __ldg(gsp + 2 * q);
+                s_spot_b[q] = __ldg(gsp + 2 * q + 1);
+            }
+            __syncthreads();
+            if (!any) continue;
+            float accp[kPbVoxY], acch[kPbVoxY];
+#pragma unroll
+            for (int v = 0; v < kPbVoxY; ++v) accp[v] = acch[v] = 0.f;
+#pragma unroll 4
+            for (int q = 0; q < cn; ++q) {
+                const float4 a = s_spot_a[q];
+                const float4 b = s_spot_b[q];
+#pragma unroll
+                for (int v = 0; v < kPbVoxY; ++v) {
+                    const float rx = hx[v] - a.x;
+                    const float ry = hy[v] - a.y;
+                    const float ray2 = fmaf(rx, rx, fmaf(ry, ry, hz2[v]));
+                    const float dot = fmaf(b.x, rx, fmaf(b.y, ry, -hz[v]));
+                    const float r2 = fmaf(-dot, dot * b.z, ray2);
+                    accp[v] = fmaf(a.z, fast_exp2(pv[v].ps2 * r2), accp[v]);
+                    acch[v] = fmaf(a.z, fast_exp2(pv[v].hs2 * r2), acch[v]);
+                }
+            }
+#pragma unroll
+            for (int v = 0; v < kPbVoxY; ++v) {
+                if (act[v]) acc[v] += fmaf(pv[v].pf, accp[v], pv[v].hf * acch[v]);
+            }
+        }
+    }
+
+#pragma unroll
+    for (int v = 0; v < kPbVoxY; ++v) {
+        const int j = j0 + v * kPbThreadsY;
+        if (inside[v]) dose[(long long)i + (long long)g.nx * (j + (long long)g.ny * k)] = acc[v];
+    }
+}
+
+void launch_pencil_beam(DeviceContext &ctx, const Grid &g, const Frame &f, const ProtonTables &t,
+                        const float *wet_s, float *dose, cudaStream_t s) {
+    const size_t smem = 2 * kPbSpotChunk * sizeof(float4) + 3 * (size_t)t.lut_len * sizeof(float);
+    static bool attr_set[64] = {false};
+    if (smem > 48 * 1024) {
+        if (ctx.device < 64 && !attr_set[ctx.device]) {
+            DC_CUDA(cudaFuncSetAttribute(pencil_beam_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         200 * 1024));
+            attr_set[ctx.device] = true;
+        }
+    }
+    dim3 block(kPbThreadsX, kPbThreadsY, 1);
+    dim3 grid((unsigned)((g.nx + kPbThreadsX - 1) / kPbThreadsX),
+              (unsigned)((g.ny + kPbThreadsY * kPbVoxY - 1) / (kPbThreadsY * kPbVoxY)), (unsigned)g.nz);
+    KernelTimer kt(ctx, "pencil_beam", s);
+    pencil_beam_kernel<<<grid, block, smem, s>>>(g, f, t, wet_s, dose);
+    check_launch("pencil_beam_kernel");
+}
+
+}  // namespace dc

@@ -1,0 +1,274 @@
+// dc_runtime.cu — device contexts, cached buffers and textures, profiler.
+#include "dc_runtime.cuh"
+#include "dc_common.cuh"
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+
+#include "../../include/dosecuda.h"
+
+namespace dc {
+
+static thread_local std::string g_last_error;
+
+void set_last_error(const std::string &msg) { g_last_error = msg; }
+const char *last_error_cstr() { return g_last_error.c_str(); }
+
+void throw_cuda(cudaError_t e, const char *what) {
+    // The reference reports "CUDA error: <cudaGetErrorString>" (dosemodule.cu:195).
+    std::string m = cudaGetErrorString(e);
+    m += " (";
+    m += what;
+    m += ")";
+    throw Error(DC_ERR_CUDA, m);
+}
+
+void check_launch(const char *kernel) {
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) throw_cuda(e, kernel);
+}
+
+// ---------------------------------------------------------------------------
+void *DeviceBuffer::ensure(size_t n) {
+    if (n <= bytes && ptr) return ptr;
+    release();
+    size_t want = n < 256 ? 256 : n;
+    void *p = nullptr;
+    DC_CUDA(cudaMalloc(&p, want));
+    ptr = p;
+    bytes = want;
+    return ptr;
+}
+
+void DeviceBuffer::release() {
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    bytes = 0;
+}
+
+void *PinnedBuffer::ensure(size_t n) {
+    if (n <= bytes && ptr) return ptr;
+    release();
+    size_t want = n < 4096 ? 4096 : n;
+    void *p = nullptr;
+    DC_CUDA(cudaMallocHost(&p, want));
+    ptr = p;
+    bytes = want;
+    return ptr;
+}
+
+void PinnedBuffer::release() {
+    if (ptr) cudaFreeHost(ptr);
+    ptr = nullptr;
+    bytes = 0;
+}
+
+// ---------------------------------------------------------------------------
+void VolumeArray::ensure(int nx_, int ny_, int nz_, bool want_surface) {
+    if (arr && nx_ == nx && ny_ == ny && nz_ == nz && (surface || !want_surface)) return;
+    release();
+    cudaChannelFormatDesc ch = cudaCreateChannelDesc<float>();
+    cudaExtent ext = make_cudaExtent((size_t)nx_, (size_t)ny_, (size_t)nz_);
+    unsigned flags = want_surface ? cudaArraySurfaceLoadStore : cudaArrayDefault;
+    DC_CUDA(cudaMalloc3DArray(&arr, &ch, ext, flags));
+    nx = nx_;
+    ny = ny_;
+    nz = nz_;
+    surface = want_surface;
+    if (want_surface) {
+        cudaResourceDesc rd{};
+        rd.resType = cudaResourceTypeArray;
+        rd.res.array.array = arr;
+        DC_CUDA(cudaCreateSurfaceObject(&surf, &rd));
+    }
+}
+
+cudaTextureObject_t VolumeArray::texture(float border) {
+    auto it = tex.find(border);
+    if (it != tex.end()) return it->second;
+    // Same sampler state as the reference (TextureClasses.cu:5-38): border
+    // addressing on all axes, hardware linear filtering, unnormalised
+    // coordinates, element-type reads.
+    cudaResourceDesc rd{};
+    rd.resType = cudaResourceTypeArray;
+    rd.res.array.array = arr;
+    cudaTextureDesc td{};
+    td.addressMode[0] = cudaAddressModeBorder;
+    td.addressMode[1] = cudaAddressModeBorder;
+    td.addressMode[2] = cudaAddressModeBorder;
+    td.filterMode = cudaFilterModeLinear;
+    td.readMode = cudaReadModeElementType;
+    td.borderColor[0] = border;
+    td.normalizedCoords = 0;
+    cudaTextureObject_t t = 0;
+    DC_CUDA(cudaCreateTextureObject(&t, &rd, &td, nullptr));
+    tex[border] = t;
+    return t;
+}
+
+void VolumeArray::release() {
+    for (auto &kv : tex) cudaDestroyTextureObject(kv.second);
+    tex.clear();
+    if (surf) cudaDestroySurfaceObject(surf);
+    surf = 0;
+    if (arr) cudaFreeArray(arr);
+    arr = nullptr;
+    nx = ny = nz = 0;
+    surface = false;
+}
+
+// ---------------------------------------------------------------------------
+DeviceContext::DeviceContext(int dev) : device(dev) {
+    DC_CUDA(cudaSetDevice(dev));
+    DC_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    DC_CUDA(cudaEventCreateWithFlags(&pin_free, cudaEventDisableTiming));
+    DC_CUDA(cudaEventCreateWithFlags(&last_use, cudaEventDisableTiming));
+}
+
+void DeviceContext::begin_call(cudaStream_t s) { DC_CUDA(cudaStreamWaitEvent(s, last_use, 0)); }
+
+void DeviceContext::end_call(cudaStream_t s) { DC_CUDA(cudaEventRecord(last_use, s)); }
+
+DeviceContext::~DeviceContext() { release_all(); }
+
+void DeviceContext::release_all() {
+    cudaSetDevice(device);
+    if (stream) cudaStreamSynchronize(stream);
+    wet_raw.release();
+    vol_a.release();
+    vol_b.release();
+    vol_c.release();
+    electron.release();
+    small.release();
+    lut.release();
+    tables.release();
+    density.release();
+    terma.release();
+    pin_small.release();
+    for (auto &p : pending) {
+        event_pool.push_back(p.a);
+        event_pool.push_back(p.b);
+    }
+    pending.clear();
+    for (auto e : event_pool) cudaEventDestroy(e);
+    event_pool.clear();
+    if (pin_free) cudaEventDestroy(pin_free);
+    if (last_use) cudaEventDestroy(last_use);
+    pin_free = last_use = nullptr;
+    if (stream) cudaStreamDestroy(stream);
+    stream = nullptr;
+}
+
+cudaEvent_t DeviceContext::take_event() {
+    if (!event_pool.empty()) {
+        cudaEvent_t e = event_pool.back();
+        event_pool.pop_back();
+        return e;
+    }
+    cudaEvent_t e;
+    DC_CUDA(cudaEventCreate(&e));
+    return e;
+}
+
+void DeviceContext::prof_begin(const char *name, cudaStream_t s, cudaEvent_t *a, cudaEvent_t *b) {
+    *a = take_event();
+    *b = take_event();
+    pending.push_back({name, *a, *b});
+    DC_CUDA(cudaEventRecord(*a, s));
+}
+
+void DeviceContext::prof_end(cudaEvent_t b, cudaStream_t s) { cudaEventRecord(b, s); }
+
+void DeviceContext::prof_collect() {
+    DC_CUDA(cudaSetDevice(device));
+    for (auto &p : pending) {
+        DC_CUDA(cudaEventSynchronize(p.b));
+        float ms = 0.f;
+        DC_CUDA(cudaEventElapsedTime(&ms, p.a, p.b));
+        auto &e = profile[p.name];
+        e.launches += 1;
+        e.total_ms += ms;
+        event_pool.push_back(p.a);
+        event_pool.push_back(p.b);
+    }
+    pending.clear();
+}
+
+// ---------------------------------------------------------------------------
+static std::mutex g_ctx_mu;
+static std::map<int, std::unique_ptr<DeviceContext>> g_ctx;
+
+DeviceContext &context(int device) {
+    int count = 0;
+    cudaError_t e = cudaGetDeviceCount(&count);
+    if (e != cudaSuccess) throw_cuda(e, "cudaGetDeviceCount");
+    if (device < 0 || device >= count) {
+        throw Error(DC_ERR_CUDA, std::string(cudaGetErrorString(cudaErrorInvalidDevice)) +
+                                     " (gpu_id " + std::to_string(device) + " of " +
+                                     std::to_string(count) + " devices)");
+    }
+    std::lock_guard<std::mutex> lk(g_ctx_mu);
+    auto it = g_ctx.find(device);
+    if (it == g_ctx.end()) {
+        it = g_ctx.emplace(device, std::unique_ptr<DeviceContext>(new DeviceContext(device))).first;
+    }
+    DC_CUDA(cudaSetDevice(device));
+    return *it->second;
+}
+
+void release_context(int device) {
+    std::lock_guard<std::mutex> lk(g_ctx_mu);
+    auto it = g_ctx.find(device);
+    if (it != g_ctx.end()) {
+        std::lock_guard<std::mutex> lk2(it->second->mu);
+        it->second->release_all();
+        g_ctx.erase(it);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Host geometry (reference CudaBeam ctor, CudaClasses.cu:17-51; IMRTBeam ctor
+// IMRTClasses.cu:30-39; gantry offset and isocentre shift dosemodule.cu:148-164).
+Frame make_frame(const float iso[3], const float origin[3], double gantry_deg, double couch_deg,
+                 double collimator_deg, float src_dist) {
+    Frame f;
+    f.isox = iso[0] - origin[0];
+    f.isoy = iso[1] - origin[1];
+    f.isoz = iso[2] - origin[2];
+    const float gantry = fmodf((float)(gantry_deg + 180.0f), 360.0f);
+    const float couch = (float)couch_deg;
+    const float coll = (float)collimator_deg;
+    const float ga = gantry * CUDART_PI_F / 180.0f;
+    const float ta = couch * CUDART_PI_F / 180.0f;
+    const float ca = coll * CUDART_PI_F / 180.0f;
+    f.sga = sinf(ga);
+    f.cga = cosf(ga);
+    f.sta = sinf(ta);
+    f.cta = cosf(ta);
+    f.sca = sinf(ca);
+    f.cca = cosf(ca);
+    const float xg = -src_dist * f.sga;
+    const float yg = src_dist * f.cga;
+    f.srcx = xg * f.cta;
+    f.srcy = yg;
+    f.srcz = -xg * f.sta;
+    return f;
+}
+
+Grid make_grid(int nz, int ny, int nx, const float spacing[3]) {
+    Grid g;
+    g.nx = nx;
+    g.ny = ny;
+    g.nz = nz;
+    g.sx = spacing[0];
+    g.sy = spacing[1];
+    g.sz = spacing[2];
+    g.inv_sx = 1.0f / g.sx;
+    g.inv_sy = 1.0f / g.sy;
+    g.inv_sz = 1.0f / g.sz;
+    return g;
+}
+
+}  // namespace dc

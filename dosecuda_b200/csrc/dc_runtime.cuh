@@ -1,0 +1,145 @@
+// dc_runtime.cuh — per-device runtime of the DoseCUDA B200 engines.
+//
+// The reference allocates, uploads and frees everything on every call
+// (MemoryClasses.h:85-137, TextureClasses.cu:44-59).  Here each device gets
+// one long-lived context holding:
+//  * a non-blocking stream for the synchronous host entry points;
+//  * grow-only device buffers (WET, dose, TERMA, spot/layer tables, LUTs);
+//  * grow-only 3D cudaArrays with texture objects (hardware trilinear
+//    filtering, border addressing) and, for the TERMA volume, a surface
+//    object so that the TERMA kernel writes the array directly;
+//  * a small kernel profiler (CUDA events per launch, opt-in).
+// Calls on one device are serialised by the context mutex.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <map>
+#include <mutex>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+namespace dc {
+
+// Error carrying the C-ABI status code.
+struct Error : std::runtime_error {
+    int code;
+    Error(int c, const std::string &m) : std::runtime_error(m), code(c) {}
+};
+
+[[noreturn]] void throw_cuda(cudaError_t e, const char *what);
+
+inline void cuda_check(cudaError_t e, const char *what) {
+    if (e != cudaSuccess) throw_cuda(e, what);
+}
+#define DC_CUDA(call) ::dc::cuda_check((call), #call)
+
+void set_last_error(const std::string &msg);
+
+// Grow-only device allocation.
+struct DeviceBuffer {
+    void *ptr = nullptr;
+    size_t bytes = 0;
+    void *ensure(size_t n);
+    void release();
+    template <class T>
+    T *as() const { return static_cast<T *>(ptr); }
+};
+
+// Grow-only pinned host allocation.
+struct PinnedBuffer {
+    void *ptr = nullptr;
+    size_t bytes = 0;
+    void *ensure(size_t n);
+    void release();
+};
+
+// A 3D float (1 channel) cudaArray with texture objects for a set of border
+// values, and optionally a surface object.
+struct VolumeArray {
+    cudaArray_t arr = nullptr;
+    int nx = 0, ny = 0, nz = 0;
+    bool surface = false;
+    cudaSurfaceObject_t surf = 0;
+    std::map<float, cudaTextureObject_t> tex;  // border value -> linear-filter texture
+
+    // (Re)allocate for the given extent; keeps the array when it matches.
+    void ensure(int nx_, int ny_, int nz_, bool want_surface);
+    cudaTextureObject_t texture(float border);
+    void release();
+};
+
+struct ProfileEntry {
+    int launches = 0;
+    double total_ms = 0.0;
+};
+
+class DeviceContext {
+   public:
+    explicit DeviceContext(int device);
+    ~DeviceContext();
+
+    int device;
+    std::mutex mu;
+    cudaStream_t stream = nullptr;  // for the host (synchronous) entry points
+
+    DeviceBuffer wet_raw;     // unsmoothed WET (cm)
+    DeviceBuffer vol_a;       // generic volume scratch (input staging)
+    DeviceBuffer vol_b;       // generic volume scratch (output)
+    DeviceBuffer vol_c;       // generic volume scratch (second output)
+    DeviceBuffer electron;    // electron contamination term
+    DeviceBuffer small;       // per-call small device tables (cone directions)
+    DeviceBuffer lut;         // proton LUT rows uploaded by the host entry point
+    DeviceBuffer tables;      // proton layer + spot tables
+    VolumeArray density;      // density / RLSP texture
+    VolumeArray terma;        // TERMA texture (surface-writable)
+    PinnedBuffer pin_small;   // staging for per-call tables
+    cudaEvent_t pin_free = nullptr;  // recorded after the last copy out of pin_small
+    cudaEvent_t last_use = nullptr;  // recorded after the last enqueued call
+
+    // Orders a call on stream s after every earlier call on this device
+    // (the cached scratch buffers are shared), and marks its end.
+    void begin_call(cudaStream_t s);
+    void end_call(cudaStream_t s);
+
+    // Profiler.
+    bool profiling = false;
+    struct Pending {
+        std::string name;
+        cudaEvent_t a, b;
+    };
+    std::vector<Pending> pending;
+    std::vector<cudaEvent_t> event_pool;
+    std::map<std::string, ProfileEntry> profile;
+    void prof_begin(const char *name, cudaStream_t s, cudaEvent_t *a, cudaEvent_t *b);
+    void prof_end(cudaEvent_t b, cudaStream_t s);
+    void prof_collect();  // synchronises the device
+    void release_all();
+
+   private:
+    cudaEvent_t take_event();
+};
+
+// Returns the context for `device` (created on first use) with the device
+// made current.  Throws Error(DC_ERR_VALUE) for an invalid ordinal.
+DeviceContext &context(int device);
+void release_context(int device);
+
+// RAII bracket for a profiled kernel launch on stream s.
+struct KernelTimer {
+    DeviceContext &ctx;
+    cudaStream_t s;
+    cudaEvent_t a = nullptr, b = nullptr;
+    KernelTimer(DeviceContext &c, const char *name, cudaStream_t st) : ctx(c), s(st) {
+        if (ctx.profiling) ctx.prof_begin(name, s, &a, &b);
+    }
+    ~KernelTimer() {
+        if (b) ctx.prof_end(b, s);
+    }
+};
+
+// Throws Error(DC_ERR_CUDA) if the last launch failed.
+void check_launch(const char *kernel);
+
+}  // namespace dc

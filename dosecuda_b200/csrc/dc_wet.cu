@@ -1,0 +1,103 @@
+// dc_wet.cu — radiological depth: per-voxel ray march to the source and the
+// proton beam's-eye-view smoothing.
+//
+// wet_march_kernel restates rayTraceKernel (CudaClasses.cu:180-228): from
+// each voxel centre, 1 mm steps towards the source, hardware-trilinear
+// density samples, WET(cm) = -0.05 + sum 0.1*max(rho,0) until the sample's
+// texture coordinate leaves [0,n).  wet_smooth_kernel restates
+// smoothRayKernel (IMPTClasses.cu:139-202): the mean of the voxel's WET and
+// the nearest-voxel WET at radii 1,2,.. mm (r < min(10*WET, 10)) along six
+// BEV directions.
+//
+// B200 mapping: one thread per voxel with a warp covering 32 consecutive x
+// voxels (coalesced loads/stores; the 32 rays of a warp march side by side so
+// their texture samples share cache lines), blocks of 32x4 voxels.  The march
+// is bound by the texture unit's trilinear fetch rate, one fetch per 1 mm
+// sample.
+#include "dc_common.cuh"
+#include "dc_runtime.cuh"
+#include "dc_kernels.cuh"
+
+namespace dc {
+
+__global__ void __launch_bounds__(128) wet_march_kernel(Grid g, Frame f, cudaTextureObject_t density,
+                                                        float *__restrict__ wet) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int k = blockIdx.z;
+    if (i >= g.nx || j >= g.ny) return;
+
+    const float3 p = voxel_xyz(g, f, i, j, k);
+    const float3 u = unit_to_source(f, p);
+
+    float wet_sum = -0.05f;
+    float t = 0.0f;
+    // The samples inside the volume form a prefix of t = 0,1,2,... (each
+    // coordinate is monotonic in t), so the loop stops at the first exit.
+    while (true) {
+        float3 q;
+        q.x = fmaf(u.x, t, p.x);
+        q.y = fmaf(u.y, t, p.y);
+        q.z = fmaf(u.z, t, p.z);
+        const float3 tc = tex_coord(g, f, q);
+        if (!tex_inside(g, tc)) break;
+        const float rho = tex3D<float>(density, tc.x, tc.y, tc.z);
+        wet_sum = fmaf(fmaxf(rho, 0.0f), 0.1f, wet_sum);
+        t += 1.0f;
+    }
+    wet[(long long)i + (long long)g.nx * (j + (long long)g.ny * k)] = wet_sum;
+}
+
+__global__ void __launch_bounds__(128) wet_smooth_kernel(Grid g, Frame f, const float *__restrict__ wet,
+                                                         float *__restrict__ wet_s) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int k = blockIdx.z;
+    if (i >= g.nx || j >= g.ny) return;
+
+    const long long v = (long long)i + (long long)g.nx * (j + (long long)g.ny * k);
+    const float3 p = voxel_xyz(g, f, i, j, k);
+    const float3 h = image_to_head<false>(f, p);
+    const float c = __ldg(wet + v);
+    const float rmax = c * 10.0f;
+    float sum = c;
+    int n = 1;
+    for (int d = 0; d < 6; ++d) {
+        float s, co;
+        sincosf((float)d * CUDART_PI_F / 3.0f, &s, &co);
+        for (float dr = 1.0f; dr < rmax && dr < 10.0f; dr += 1.0f) {
+            float3 hc = make_float3(h.x + dr * co, h.y + dr * s, h.z);
+            const float3 q = head_to_image<false>(f, hc);
+            // Nearest voxel (CudaClasses.cuh:112-116): division, as the reference.
+            const int qi = (int)roundf((q.x + f.isox) / g.sx);
+            const int qj = (int)roundf((q.y + f.isoy) / g.sy);
+            const int qk = (int)roundf((q.z + f.isoz) / g.sz);
+            if ((unsigned)qi < (unsigned)g.nx && (unsigned)qj < (unsigned)g.ny &&
+                (unsigned)qk < (unsigned)g.nz) {
+                sum += __ldg(wet + (long long)qi + (long long)g.nx * (qj + (long long)g.ny * qk));
+                n += 1;
+            }
+        }
+    }
+    wet_s[v] = sum / (float)n;
+}
+
+static dim3 volume_grid(const Grid &g) {
+    return dim3((unsigned)((g.nx + 31) / 32), (unsigned)((g.ny + 3) / 4), (unsigned)g.nz);
+}
+
+void launch_wet_march(DeviceContext &ctx, const Grid &g, const Frame &f, cudaTextureObject_t density,
+                      float *wet, cudaStream_t s) {
+    KernelTimer kt(ctx, "wet_march", s);
+    wet_march_kernel<<<volume_grid(g), dim3(32, 4, 1), 0, s>>>(g, f, density, wet);
+    check_launch("wet_march_kernel");
+}
+
+void launch_wet_smooth(DeviceContext &ctx, const Grid &g, const Frame &f, const float *wet, float *wet_s,
+                       cudaStream_t s) {
+    KernelTimer kt(ctx, "wet_smooth", s);
+    wet_smooth_kernel<<<volume_grid(g), dim3(32, 4, 1), 0, s>>>(g, f, wet, wet_s);
+    check_launch("wet_smooth_kernel");
+}
+
+}  // namespace dc

@@ -1,0 +1,202 @@
+/*
+ * dosecuda.h — C ABI of the B200 (sm_100a) DoseCUDA dose engines.
+ *
+ * This is the drop-in boundary for the reference's `dose_kernels` CPython
+ * extension (DoseCUDA/dose_kernels/dosemodule.cu).  Each host entry point
+ * below replaces one function of that module's method table
+ * (dosemodule.cu:560-580) and keeps its argument meaning, its output, and its
+ * error classes; the Python shim `dosecuda_b200/dose_kernels.py` maps the
+ * reference's duck-typed (model, volume, beam, gpu_id) objects onto these
+ * plain-pointer calls.
+ *
+ * Conventions
+ *  - Volumes are C-contiguous float32 arrays of shape (nz, ny, nx), index
+ *    i + nx*(j + ny*k)  (reference CudaClasses.cuh:96-98).
+ *  - spacing/origin/iso are in mm, in (x, y, z) order.  The engines accept
+ *    three spacings; the reference itself only reads spacing[0]
+ *    (dosemodule.cu:146,300,471), and the `dose_kernels` shim passes
+ *    spacing[0] three times to reproduce that.
+ *  - Angles are in degrees, as the caller gives them; the +180 degree gantry
+ *    offset of the reference (dosemodule.cu:152,304,477) is applied inside.
+ *    The gantry angle is a double because the reference forms
+ *    fmodf(gantry + 180, 360) from the Python float before rounding.
+ *  - Every function returns DC_OK (0) or an error code; dc_last_error()
+ *    returns the message of the calling thread's last failure.
+ *  - Host entry points (no suffix) take host pointers and are synchronous,
+ *    like the reference.  The *_dev entry points take device pointers and a
+ *    cudaStream_t (passed as void*; NULL = legacy default stream), enqueue
+ *    the work and return without synchronising.
+ *  - Outputs are caller-owned buffers of nz*ny*nx floats.
+ */
+#ifndef DOSECUDA_H
+#define DOSECUDA_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DC_OK 0
+#define DC_ERR_VALUE 1   /* bad argument: the reference raises ValueError    */
+#define DC_ERR_MEMORY 2  /* host allocation failed: MemoryError            */
+#define DC_ERR_CUDA 3    /* CUDA runtime/launch failure: RuntimeError       */
+
+/* Photon beam model: the scalar and 1-D array attributes that the reference
+ * reads from an IMRTPhotonEnergy object (dosemodule.cu:400-437).  The CCCS
+ * kernel table is passed as its six logical columns (kernel.csv: theta in
+ * degrees, Am, am, Bm, bm, ray_length in cm), n_cones rows each; the
+ * reference reads the same numbers column-major from the pandas-built array
+ * (IMRTClasses.cu:292-297). */
+typedef struct dc_photon_model {
+    int n_profile_points;
+    const float *profile_radius;        /* mm, ascending            */
+    const float *profile_intensities;
+    const float *profile_softening;
+    int n_spectral_energies;
+    const float *spectrum_attenuation_coefficients;  /* 1/cm */
+    const float *spectrum_primary_weights;
+    const float *spectrum_scatter_weights;
+    float mu_calibration;
+    float primary_source_distance;      /* mm */
+    float scatter_source_distance;      /* mm */
+    float primary_source_size;          /* mm */
+    float scatter_source_size;          /* mm */
+    float mlc_distance;                 /* mm */
+    float scatter_source_weight;
+    float electron_attenuation;
+    float electron_source_weight;
+    float electron_fitted_dmax;
+    float jaw_transmission;             /* parsed, unused (as the reference) */
+    float mlc_transmission;             /* parsed, unused (as the reference) */
+    int has_xjaws;                      /* parsed, unused (as the reference) */
+    int has_yjaws;                      /* parsed, unused (as the reference) */
+    int n_cones;                        /* rows of the kernel table (6)      */
+    const float *kernel_theta_deg;
+    const float *kernel_Am;
+    const float *kernel_am;
+    const float *kernel_Bm;
+    const float *kernel_bm;
+    const float *kernel_ray_length;     /* cm */
+} dc_photon_model;
+
+/* One photon control point (reference IMRTControlPoint, plan_imrt.py:95-105).
+ * MLC leaf pairs are passed as four logical columns of n_mlc_pairs values:
+ * x1, x2 (leaf tips, mm at isocentre), y_offset and y_width (mm); the
+ * reference reads them the same way (dosemodule.cu:228-240). */
+typedef struct dc_control_point {
+    float iso[3];
+    float mu;
+    double gantry_deg;  /* double: the reference adds 180 in double before
+                           rounding to float (dosemodule.cu:477) */
+    float collimator_deg;
+    float couch_deg;
+    int n_mlc_pairs;
+    const float *mlc_x1;
+    const float *mlc_x2;
+    const float *mlc_y_offset;
+    const float *mlc_y_width;
+} dc_control_point;
+
+/* ------------------------------------------------------------------ */
+/* Library                                                             */
+/* ------------------------------------------------------------------ */
+
+/* Message of the calling thread's last failed call ("" if none). */
+const char *dc_last_error(void);
+
+/* ABI version (major*10000 + minor*100 + patch). */
+int dc_version(void);
+
+/* Number of CUDA devices visible (0 when none), or -1 on a driver error. */
+int dc_device_count(void);
+
+/* Free the cached device buffers, textures and streams held for gpu_id. */
+int dc_release_device(int gpu_id);
+
+/* Kernel timing: when enabled, every kernel the library launches is
+ * bracketed by CUDA events on its own stream.  dc_profile_read synchronises
+ * the device and returns, per kernel name, the launch count and the summed
+ * device time (ms).  Returns the number of kernels written (<= max). */
+int dc_profile_enable(int gpu_id, int on);
+int dc_profile_reset(int gpu_id);
+int dc_profile_read(int gpu_id, int max, const char **names, int *launches, double *total_ms);
+
+/* ------------------------------------------------------------------ */
+/* Proton: water-equivalent thickness (WET) ray trace + BEV smoothing   */
+/* Replaces dose_kernels.proton_raytrace_cuda                           */
+/* (dosemodule.cu:104-201 -> IMPTClasses.cu:274-299).                   */
+/* Output: smoothed WET in cm.                                          */
+/* ------------------------------------------------------------------ */
+int dc_proton_raytrace(int gpu_id,
+                       const float *rlsp, int nz, int ny, int nx,
+                       const float spacing[3], const float origin[3],
+                       const float iso[3], double gantry_deg, float couch_deg,
+                       float vsadx, float vsady,
+                       float *wet_out);
+
+int dc_proton_raytrace_dev(int gpu_id,
+                           const float *rlsp_dev, int nz, int ny, int nx,
+                           const float spacing[3], const float origin[3],
+                           const float iso[3], double gantry_deg, float couch_deg,
+                           float vsadx, float vsady,
+                           float *wet_out_dev, void *stream);
+
+/* ------------------------------------------------------------------ */
+/* Proton: double-Gaussian pencil-beam dose from a precomputed WET      */
+/* Replaces dose_kernels.proton_spot_cuda                               */
+/* (dosemodule.cu:243-374 -> IMPTClasses.cu:301-340).                   */
+/*  divergence_params : [n_energies][dvp_len] = energy, R80, A, B, C    */
+/*  lut_*             : [n_energies][lut_len] depth (mm), sigma (mm),   */
+/*                      IDD; the reference uses lut_len = 400           */
+/*  spots             : [n_spots][4] = x (mm), y (mm), MU, energy_id    */
+/* Output: dose (Gy for the tables' calibration), accumulated over the  */
+/* spots of the beam.                                                   */
+/* ------------------------------------------------------------------ */
+int dc_proton_spot(int gpu_id,
+                   const float *wet, int nz, int ny, int nx,
+                   const float spacing[3], const float origin[3],
+                   const float iso[3], double gantry_deg, float couch_deg,
+                   float vsadx, float vsady,
+                   const float *divergence_params, int n_energies, int dvp_len,
+                   const float *lut_depths, const float *lut_sigmas,
+                   const float *lut_idds, int lut_len,
+                   const float *spots, int n_spots,
+                   float *dose_out);
+
+/* Device variant.  wet/dose/LUT pointers are device pointers; `spots` is a
+ * HOST array (the layer table is built on the host, as the reference does
+ * in dosemodule.cu:204-225 and IMPTClasses.cu:37-67). */
+int dc_proton_spot_dev(int gpu_id,
+                       const float *wet_dev, int nz, int ny, int nx,
+                       const float spacing[3], const float origin[3],
+                       const float iso[3], double gantry_deg, float couch_deg,
+                       float vsadx, float vsady,
+                       const float *divergence_params, int n_energies, int dvp_len,
+                       const float *lut_depths_dev, const float *lut_sigmas_dev,
+                       const float *lut_idds_dev, int lut_len,
+                       const float *spots, int n_spots,
+                       float *dose_out_dev, void *stream);
+
+/* ------------------------------------------------------------------ */
+/* Photon: ray trace + TERMA + collapsed-cone convolution/superposition */
+/* Replaces dose_kernels.photon_dose_cuda                               */
+/* (dosemodule.cu:377-557 -> IMRTClasses.cu:353-405).                   */
+/* Output: dose for one control point (before the output factor, which  */
+/* the plan layer applies, plan_imrt.py:151-153).                       */
+/* ------------------------------------------------------------------ */
+int dc_photon_dose(int gpu_id,
+                   const float *density, int nz, int ny, int nx,
+                   const float spacing[3], const float origin[3],
+                   const dc_photon_model *model, const dc_control_point *cp,
+                   float *dose_out);
+
+int dc_photon_dose_dev(int gpu_id,
+                       const float *density_dev, int nz, int ny, int nx,
+                       const float spacing[3], const float origin[3],
+                       const dc_photon_model *model, const dc_control_point *cp,
+                       float *dose_out_dev, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DOSECUDA_H */
