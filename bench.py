@@ -35,6 +35,9 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 PEAKS_FALLBACK = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
+# DRAM bytes (read + write) per launch from one ncu --set full capture of each
+# dominant kernel on these workloads (profiles/*.md)
+NCU_TRAFFIC = {"cccs": 21117952, "pencil_beam": 3613952}
 SM_COUNT = 148
 FP32_LANES_PER_SM = 128
 
@@ -92,7 +95,7 @@ class ClockSampler:
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.Q,
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self._t = threading.Thread(target=self._read, daemon=True)
             self._t.start()
@@ -238,8 +241,8 @@ def run_mine(args, ws, rank, local, dist_mod):
     torch.cuda.synchronize()
     barrier(dist_mod)
     torch.cuda.synchronize()
-    with ClockSampler(local) as clk:
-        t_ms = time_steps(step_x, args.steps, flush)
+    clk = ClockSampler(local).__enter__()  # sampled across all timed regions below
+    t_ms = time_steps(step_x, args.steps, flush)
     torch.cuda.synchronize()
     barrier(dist_mod)
     t_ms = aggregate_max(t_ms, dist_mod)
@@ -265,7 +268,9 @@ def run_mine(args, ws, rank, local, dist_mod):
     fp32_peak = SM_COUNT * FP32_LANES_PER_SM * 2 * pk.get("sm_max_mhz", 1965.0) * 1e6 / 1e12
     achieved_tf = samples * flops_per_sample / (cccs_avg_ms * 1e-3) / 1e12
     nvox = density.size
-    cccs_bytes = nvox * 4 * 2 + n_active * 4  # electron + dose + TERMA mask read (algorithmic)
+    # algorithmic bytes: the (TERMA, density) float2 volume read once, the
+    # electron term read once, the dose written once = 16 B per voxel
+    cccs_bytes = nvox * 16
 
     # e2e through the drop-in API (pinned host input, H2D + D2H per call)
     pinned = torch.from_numpy(density).pin_memory()
@@ -304,6 +309,7 @@ def run_mine(args, ws, rank, local, dist_mod):
     torch.cuda.synchronize()
     barrier(dist_mod)
     tp_ms = time_steps(step_p, args.steps, flush)
+    clk.__exit__(None, None, None)
     barrier(dist_mod)
     tp_ms = aggregate_max(tp_ms, dist_mod)
     spots_per_s = n_spots * args.steps * ws / (tp_ms * 1e-3)
@@ -436,7 +442,9 @@ def main_mine(args):
                 "hbm": {"achieved_gbs": round(r["cccs_bytes"] / (r["cccs_avg_ms"] * 1e-3) / 1e9, 2),
                         "peak_gbs": hbm, "frac": round(r["cccs_bytes"] / (r["cccs_avg_ms"] * 1e-3) / 1e9 / hbm, 5),
                         "peak_kind": r["pk_kind"]},
-                "traffic": None,
+                # dram__bytes_read.sum + dram__bytes_write.sum of one ncu capture
+                # of this kernel on this workload (profiles/cccs_photon_small.md)
+                "traffic": NCU_TRAFFIC["cccs"],
             },
             "kernels": {k: {"launches": v[0], "total_ms": round(v[1], 4)} for k, v in r["prof_x"].items()},
             "gpu_launches": x_launch_per_step * args.steps,
@@ -460,7 +468,7 @@ def main_mine(args):
                              "frac": round(r["pb_flops"] / (r["pb_avg_ms"] * 1e-3) / 1e12 / r["fp32_peak"], 4),
                              "work": f"{r['pairs']} (voxel, spot) pairs x 20 FP32 flops (+2 SFU exp each)",
                              "pairs_per_s": round(r["pairs"] / (r["pb_avg_ms"] * 1e-3), 1),
-                             "kernel_ms": round(r["pb_avg_ms"], 4), "traffic": None},
+                             "kernel_ms": round(r["pb_avg_ms"], 4), "traffic": NCU_TRAFFIC["pencil_beam"]},
                 "kernels": {k: {"launches": v[0], "total_ms": round(v[1], 4)} for k, v in r["prof_p"].items()},
                 "gpu_launches": p_launch_per_step * args.steps,
                 "cpu_baseline": cpu_p,

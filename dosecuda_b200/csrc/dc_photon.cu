@@ -64,8 +64,12 @@ __device__ __forceinline__ float head_transmission(const PhotonParams &P, float3
     return trans;
 }
 
+// Writes (TERMA, density) of each voxel as one float2 texel of the CCCS
+// volume; the density is the input texture read at the texel centre, where
+// linear filtering returns the stored value unchanged.
 __global__ void __launch_bounds__(128) terma_kernel(Grid g, Frame f, PhotonParams P, const float *__restrict__ wet,
-                                                    cudaSurfaceObject_t terma_surf, float *__restrict__ electron) {
+                                                    cudaTextureObject_t dens_tex, cudaSurfaceObject_t td_surf,
+                                                    float *__restrict__ electron) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
     const int k = blockIdx.z;
@@ -111,7 +115,8 @@ __global__ void __launch_bounds__(128) terma_kernel(Grid g, Frame f, PhotonParam
     const float e_dmax = expf(-P.ea * P.efd);
     const float elec = fmaxf(0.0f, (expf(-P.ea * w) - e_dmax) / (1.0f - e_dmax));
     const float T = oaf * ((1.0f - P.ssw) * tp * terma + P.ssw * ts * terma);
-    surf3Dwrite(T, terma_surf, i * (int)sizeof(float), j, k);
+    const float rho = tex3D<float>(dens_tex, (float)i + 0.5f, (float)j + 0.5f, (float)k + 0.5f);
+    surf3Dwrite(make_float2(T, rho), td_surf, i * (int)sizeof(float2), j, k);
     electron[v] = P.esw * (0.4f + (0.3f * ratio)) * elec * tp;
 }
 
@@ -136,9 +141,11 @@ __global__ void cone_dirs_kernel(Frame f, CccsCones C, float4 *__restrict__ dirs
 // ---------------------------------------------------------------------------
 // CCCS
 // ---------------------------------------------------------------------------
+// td_tex: float2 (TERMA, density) texture, border (0, AIR_DENSITY) — one
+// filtered fetch serves both of the reference's textures (the same
+// coordinates and weights apply to both channels).
 __global__ void __launch_bounds__(128) cccs_kernel(Grid g, Frame f, CccsCones C, float sp_cm, float dose_scale,
-                                                   const float4 *__restrict__ dirs, cudaTextureObject_t terma_tex,
-                                                   cudaTextureObject_t dens_tex,
+                                                   const float4 *__restrict__ dirs, cudaTextureObject_t td_tex,
                                                    const float *__restrict__ electron, float *__restrict__ dose) {
     __shared__ float4 s_dir[kMaxCones * 12];
     __shared__ float s_rl10[kMaxConeSteps];
@@ -155,7 +162,7 @@ __global__ void __launch_bounds__(128) cccs_kernel(Grid g, Frame f, CccsCones C,
 
     const float3 p = voxel_xyz(g, f, i, j, k);
     const float3 tc0 = tex_coord(g, f, p);
-    if (tex3D<float>(terma_tex, tc0.x, tc0.y, tc0.z) <= 0.01f) {
+    if (tex3D<float2>(td_tex, tc0.x, tc0.y, tc0.z).x <= 0.01f) {
         dose[v] = 0.0f;
         return;
     }
@@ -200,9 +207,9 @@ __global__ void __launch_bounds__(128) cccs_kernel(Grid g, Frame f, CccsCones C,
                 q.y = fmaf(r.y, rl10, p.y);
                 q.z = fmaf(r.z, rl10, p.z);
                 const float3 tc = tex_coord(g, f, q);
-                const float Ti = tex3D<float>(terma_tex, tc.x, tc.y, tc.z);
-                float Di = tex3D<float>(dens_tex, tc.x, tc.y, tc.z);
-                Di = fmaxf(Di, kAirDensity) * sp_cm;
+                const float2 td = tex3D<float2>(td_tex, tc.x, tc.y, tc.z);
+                const float Ti = td.x;
+                const float Di = fmaxf(td.y, kAirDensity) * sp_cm;
                 const float ex = fast_exp2(nam_l2e * Di);
                 Rp = Rp * ex + (Ti * cp * (1.0f - ex));
                 Rs = Rs * (1.0f - (bm * Di)) + (Ti * Di * cs);
@@ -301,8 +308,10 @@ void run_photon_pipeline(DeviceContext &ctx, const Grid &g, const Frame &f, cons
     // The density volume is already in ctx.density; border AIR_DENSITY
     // (IMRTClasses.cu:394).
     cudaTextureObject_t dens_tex = ctx.density.texture(kAirDensity);
-    ctx.terma.ensure(g.nx, g.ny, g.nz, true);
-    cudaTextureObject_t terma_tex = ctx.terma.texture(0.0f);
+    // (TERMA, density) volume: TERMA border 0 (IMRTClasses.cu:399), density
+    // border AIR_DENSITY (:394).
+    ctx.terma.ensure(g.nx, g.ny, g.nz, true, 2);
+    cudaTextureObject_t td_tex = ctx.terma.texture(0.0f, kAirDensity);
 
     float *wet = static_cast<float *>(ctx.wet_raw.ensure((size_t)n * sizeof(float)));
     float *elec = static_cast<float *>(ctx.electron.ensure((size_t)n * sizeof(float)));
@@ -311,15 +320,15 @@ void run_photon_pipeline(DeviceContext &ctx, const Grid &g, const Frame &f, cons
     launch_wet_march(ctx, g, f, dens_tex, wet, s);
     {
         KernelTimer kt(ctx, "terma", s);
-        terma_kernel<<<vol_grid(g), dim3(32, 4, 1), 0, s>>>(g, f, P, wet, ctx.terma.surf, elec);
+        terma_kernel<<<vol_grid(g), dim3(32, 4, 1), 0, s>>>(g, f, P, wet, dens_tex, ctx.terma.surf, elec);
         check_launch("terma_kernel");
     }
     cone_dirs_kernel<<<1, kMaxCones * 12, 0, s>>>(f, C, dirs);
     check_launch("cone_dirs_kernel");
     {
         KernelTimer kt(ctx, "cccs", s);
-        cccs_kernel<<<vol_grid(g), dim3(32, 4, 1), 0, s>>>(g, f, C, g.sx / 10.0f, dose_scale, dirs, terma_tex,
-                                                           dens_tex, elec, dose_dev);
+        cccs_kernel<<<vol_grid(g), dim3(32, 4, 1), 0, s>>>(g, f, C, g.sx / 10.0f, dose_scale, dirs, td_tex, elec,
+                                                           dose_dev);
         check_launch("cccs_kernel");
     }
 }

@@ -66,10 +66,11 @@ void PinnedBuffer::release() {
 }
 
 // ---------------------------------------------------------------------------
-void VolumeArray::ensure(int nx_, int ny_, int nz_, bool want_surface) {
-    if (arr && nx_ == nx && ny_ == ny && nz_ == nz && (surface || !want_surface)) return;
+void VolumeArray::ensure(int nx_, int ny_, int nz_, bool want_surface, int channels_) {
+    if (arr && nx_ == nx && ny_ == ny && nz_ == nz && channels_ == channels && (surface || !want_surface)) return;
     release();
-    cudaChannelFormatDesc ch = cudaCreateChannelDesc<float>();
+    cudaChannelFormatDesc ch = channels_ == 2 ? cudaCreateChannelDesc<float2>() : cudaCreateChannelDesc<float>();
+    channels = channels_;
     cudaExtent ext = make_cudaExtent((size_t)nx_, (size_t)ny_, (size_t)nz_);
     unsigned flags = want_surface ? cudaArraySurfaceLoadStore : cudaArrayDefault;
     DC_CUDA(cudaMalloc3DArray(&arr, &ch, ext, flags));
@@ -85,8 +86,9 @@ void VolumeArray::ensure(int nx_, int ny_, int nz_, bool want_surface) {
     }
 }
 
-cudaTextureObject_t VolumeArray::texture(float border) {
-    auto it = tex.find(border);
+cudaTextureObject_t VolumeArray::texture(float border0, float border1) {
+    const std::pair<float, float> key(border0, border1);
+    auto it = tex.find(key);
     if (it != tex.end()) return it->second;
     // Same sampler state as the reference (TextureClasses.cu:5-38): border
     // addressing on all axes, hardware linear filtering, unnormalised
@@ -100,11 +102,12 @@ cudaTextureObject_t VolumeArray::texture(float border) {
     td.addressMode[2] = cudaAddressModeBorder;
     td.filterMode = cudaFilterModeLinear;
     td.readMode = cudaReadModeElementType;
-    td.borderColor[0] = border;
+    td.borderColor[0] = border0;
+    td.borderColor[1] = border1;
     td.normalizedCoords = 0;
     cudaTextureObject_t t = 0;
     DC_CUDA(cudaCreateTextureObject(&t, &rd, &td, nullptr));
-    tex[border] = t;
+    tex[key] = t;
     return t;
 }
 

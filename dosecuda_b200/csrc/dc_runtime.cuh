@@ -55,18 +55,19 @@ struct PinnedBuffer {
     void release();
 };
 
-// A 3D float (1 channel) cudaArray with texture objects for a set of border
-// values, and optionally a surface object.
+// A 3D float cudaArray (1 or 2 channels) with linear-filter texture objects
+// for a set of border values, and optionally a surface object.
 struct VolumeArray {
     cudaArray_t arr = nullptr;
     int nx = 0, ny = 0, nz = 0;
+    int channels = 1;
     bool surface = false;
     cudaSurfaceObject_t surf = 0;
-    std::map<float, cudaTextureObject_t> tex;  // border value -> linear-filter texture
+    std::map<std::pair<float, float>, cudaTextureObject_t> tex;  // border values -> texture
 
     // (Re)allocate for the given extent; keeps the array when it matches.
-    void ensure(int nx_, int ny_, int nz_, bool want_surface);
-    cudaTextureObject_t texture(float border);
+    void ensure(int nx_, int ny_, int nz_, bool want_surface, int channels_ = 1);
+    cudaTextureObject_t texture(float border0, float border1 = 0.0f);
     void release();
 };
 
