@@ -86,6 +86,8 @@ SIGNATURES = {
     "dc_proton_raytrace": (C.c_int, _VOL + [_F3, C.c_double, C.c_float, C.c_float, C.c_float, C.c_void_p]),
     "dc_proton_raytrace_dev": (C.c_int, _VOL + [_F3, C.c_double, C.c_float, C.c_float, C.c_float, C.c_void_p,
                                                 C.c_void_p]),
+    "dc_proton_raytrace_noalloc": (C.c_int, _VOL + [_F3, C.c_double, C.c_float, C.c_float, C.c_float,
+                                                    C.c_void_p, C.c_void_p]),
     "dc_proton_spot": (C.c_int, _VOL + [_F3, C.c_double, C.c_float, C.c_float, C.c_float,
                                         C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int,
                                         C.c_void_p, C.c_int, C.c_void_p]),

@@ -140,6 +140,23 @@ int dc_proton_raytrace_dev(int gpu_id,
                            float vsadx, float vsady,
                            float *wet_out_dev, void *stream);
 
+/* No counterpart in the reference.  Same result as dc_proton_raytrace_dev
+ * (within the rounding of its interpolation weights) for callers that
+ * cannot let the library allocate device memory: it allocates nothing.  Its
+ * only scratch is a device array of 4,194,304 floats (16 MiB) inside the
+ * library, held by every GPU that loads it until the process exits; larger
+ * volumes are rejected with DC_ERR_VALUE.  The RLSP is read from the
+ * caller's device buffer (no texture), the output goes to the caller's
+ * device buffer, work is enqueued on `stream`.  The first call on a device
+ * looks up the scratch address — make it before any stream capture.  All
+ * calls share the scratch: calls that overlap on the GPU race. */
+int dc_proton_raytrace_noalloc(int gpu_id,
+                               const float *rlsp_dev, int nz, int ny, int nx,
+                               const float spacing[3], const float origin[3],
+                               const float iso[3], double gantry_deg, float couch_deg,
+                               float vsadx, float vsady,
+                               float *wet_out_dev, void *stream);
+
 /* ------------------------------------------------------------------ */
 /* Proton: double-Gaussian pencil-beam dose from a precomputed WET      */
 /* Replaces dose_kernels.proton_spot_cuda                               */

@@ -13,6 +13,20 @@ from __future__ import annotations
 import numpy as np
 
 
+WET_MAX_CM = 0.1        # no voxel further apart than 1 mm of water
+WET_CLOSE_CM = 1e-3     # ... and 99.5 % of voxels within 0.01 mm
+WET_CLOSE_FRAC = 0.995
+
+
+def wet_close(a, b):
+    """WET (cm) agreement between two implementations of the reference's
+    sampling: the 1 mm march plus the smoothing, whose radius test
+    (r < 10 * WET) and nearest-voxel picks are knife edges, so a 1e-4 cm
+    difference can flip a few voxels' neighbour sets."""
+    d = np.abs(np.asarray(a, np.float64) - np.asarray(b, np.float64))
+    return bool(d.max() <= WET_MAX_CM and np.mean(d <= WET_CLOSE_CM) >= WET_CLOSE_FRAC)
+
+
 def dose_diff(a, b, thresh=0.10):
     a = np.asarray(a, np.float64)
     b = np.asarray(b, np.float64)
