@@ -13,19 +13,25 @@
 // cone direction tilted so that its axis points at the source.
 //
 // B200 design points:
-//  * TERMA is written straight into the surface-writable cudaArray that the
-//    CCCS kernel samples (the reference writes linear memory and copies it
-//    into a fresh array, IMRTClasses.cu:398-399).
+//  * TERMA and density are written as one float2 texel into the
+//    surface-writable cudaArray that the CCCS kernel samples, so one filtered
+//    fetch per cone sample serves both (the reference writes TERMA to linear
+//    memory, copies it into a fresh array and samples two textures,
+//    IMRTClasses.cu:398-399,423-424).
 //  * Leaf pairs whose edges are more than 4.5 source-sigmas from the voxel's
 //    projection give exactly erf = +-1 on both edges, i.e. no transmission;
 //    they are skipped without evaluating erf (open-field cost drops from
 //    4*60*2 erf per voxel to the few pairs under the penumbra).
+//  * The TERMA kernel applies the CCCS mask and lists the active voxels; the
+//    CCCS is a persistent grid-stride loop over that list, so every lane of
+//    every warp marches (masked voxels no longer idle lanes).
 //  * The 72 image-space cone directions, the per-cone step tables (the float
 //    sequence ray_length, ray_length - sp, ... >= 0 that sets each cone's
 //    sample count) and the cone coefficients are computed once per call and
 //    held in shared memory; per sample the kernel does 3 FMAs of position,
-//    two texture fetches, one SFU exponential and the two recursions.
-//  * Threads map to 32x4 voxel tiles (coalesced stores, side-by-side rays).
+//    one float2 texture fetch, one SFU exponential and the two recursions.
+//  * The TERMA kernel maps threads to 32x4 voxel tiles (coalesced stores).
+#include <algorithm>
 #include <cmath>
 #include <string>
 #include <vector>
@@ -66,10 +72,14 @@ __device__ __forceinline__ float head_transmission(const PhotonParams &P, float3
 
 // Writes (TERMA, density) of each voxel as one float2 texel of the CCCS
 // volume; the density is the input texture read at the texel centre, where
-// linear filtering returns the stored value unchanged.
+// linear filtering returns the stored value unchanged.  It also applies the
+// CCCS mask (dose 0 where TERMA <= 0.01, IMRTClasses.cu:270-273): masked
+// voxels get their zero dose here, the others are appended to `active`
+// (warp-aggregated), so the CCCS runs on full warps of active voxels only.
 __global__ void __launch_bounds__(128) terma_kernel(Grid g, Frame f, PhotonParams P, const float *__restrict__ wet,
                                                     cudaTextureObject_t dens_tex, cudaSurfaceObject_t td_surf,
-                                                    float *__restrict__ electron) {
+                                                    float *__restrict__ electron, float *__restrict__ dose,
+                                                    int *__restrict__ active, unsigned *__restrict__ n_active) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
     const int k = blockIdx.z;
@@ -118,6 +128,19 @@ __global__ void __launch_bounds__(128) terma_kernel(Grid g, Frame f, PhotonParam
     const float rho = tex3D<float>(dens_tex, (float)i + 0.5f, (float)j + 0.5f, (float)k + 0.5f);
     surf3Dwrite(make_float2(T, rho), td_surf, i * (int)sizeof(float2), j, k);
     electron[v] = P.esw * (0.4f + (0.3f * ratio)) * elec * tp;
+
+    const bool act = !(T <= 0.01f);
+    if (!act) dose[v] = 0.0f;
+    const unsigned live = __activemask();
+    const unsigned bal = __ballot_sync(live, act);
+    if (act) {
+        const int lane = threadIdx.x & 31;
+        const int leader = __ffs(bal) - 1;
+        unsigned base = 0;
+        if (lane == leader) base = atomicAdd(n_active, (unsigned)__popc(bal));
+        base = __shfl_sync(bal, base, leader);
+        active[base + __popc(bal & ((1u << lane) - 1u))] = (int)v;
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -144,29 +167,43 @@ __global__ void cone_dirs_kernel(Frame f, CccsCones C, float4 *__restrict__ dirs
 // td_tex: float2 (TERMA, density) texture, border (0, AIR_DENSITY) — one
 // filtered fetch serves both of the reference's textures (the same
 // coordinates and weights apply to both channels).
+// Persistent grid-stride loop over the active voxels listed by the TERMA
+// kernel (every lane of a warp does a full 72-direction march).
+__device__ __forceinline__ float cccs_voxel(const Grid &g, const Frame &f, const CccsCones &C, float sp_cm,
+                                            const float4 *s_dir, const float *s_rl10, cudaTextureObject_t td_tex,
+                                            float3 p);
+
 __global__ void __launch_bounds__(128) cccs_kernel(Grid g, Frame f, CccsCones C, float sp_cm, float dose_scale,
                                                    const float4 *__restrict__ dirs, cudaTextureObject_t td_tex,
-                                                   const float *__restrict__ electron, float *__restrict__ dose) {
+                                                   const float *__restrict__ electron, const int *__restrict__ active,
+                                                   const unsigned *__restrict__ n_active, float *__restrict__ dose) {
     __shared__ float4 s_dir[kMaxCones * 12];
     __shared__ float s_rl10[kMaxConeSteps];
-    const int tid = threadIdx.y * blockDim.x + threadIdx.x;
-    for (int q = tid; q < C.n_cones * 12; q += blockDim.x * blockDim.y) s_dir[q] = dirs[q];
-    for (int q = tid; q < C.total_steps; q += blockDim.x * blockDim.y) s_rl10[q] = C.rl10[q];
+    const int tid = threadIdx.x;
+    for (int q = tid; q < C.n_cones * 12; q += blockDim.x) s_dir[q] = dirs[q];
+    for (int q = tid; q < C.total_steps; q += blockDim.x) s_rl10[q] = C.rl10[q];
     __syncthreads();
 
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const int j = blockIdx.y * blockDim.y + threadIdx.y;
-    const int k = blockIdx.z;
-    if (i >= g.nx || j >= g.ny) return;
-    const long long v = (long long)i + (long long)g.nx * (j + (long long)g.ny * k);
-
-    const float3 p = voxel_xyz(g, f, i, j, k);
-    const float3 tc0 = tex_coord(g, f, p);
-    if (tex3D<float2>(td_tex, tc0.x, tc0.y, tc0.z).x <= 0.01f) {
-        dose[v] = 0.0f;
-        return;
+    const unsigned n = *n_active;
+    const int plane = g.nx * g.ny;
+    for (unsigned t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+        const int v = __ldg(active + t);
+        const int k = v / plane;
+        const int rem = v - k * plane;
+        const int j = rem / g.nx;
+        const int i = rem - j * g.nx;
+        const float3 p = voxel_xyz(g, f, i, j, k);
+        float dose_value = cccs_voxel(g, f, C, sp_cm, s_dir, s_rl10, td_tex, p);
+        dose_value += __ldg(electron + v);
+        dose[v] = (!isnan(dose_value) && dose_value >= 0.0f) ? dose_scale * dose_value : 0.0f;
     }
+}
 
+// Sum over the 6 zenith cones x 12 azimuths of the backward recursion
+// (IMRTClasses.cu:289-339) for the voxel at image position p.
+__device__ __forceinline__ float cccs_voxel(const Grid &g, const Frame &f, const CccsCones &C, float sp_cm,
+                                            const float4 *s_dir, const float *s_rl10, cudaTextureObject_t td_tex,
+                                            float3 p) {
     // kernelTilt (IMRTClasses.cu:173-203): rotate each direction by the
     // rotation taking the central axis (iso -> source) onto voxel -> source.
     const float3 uvec = unit_to_source(f, p);
@@ -217,8 +254,7 @@ __global__ void __launch_bounds__(128) cccs_kernel(Grid g, Frame f, CccsCones C,
             dose_value += am * Rp + bm * Rs;
         }
     }
-    dose_value += __ldg(electron + v);
-    dose[v] = (!isnan(dose_value) && dose_value >= 0.0f) ? dose_scale * dose_value : 0.0f;
+    return dose_value;
 }
 
 // ---------------------------------------------------------------------------
@@ -313,22 +349,34 @@ void run_photon_pipeline(DeviceContext &ctx, const Grid &g, const Frame &f, cons
     ctx.terma.ensure(g.nx, g.ny, g.nz, true, 2);
     cudaTextureObject_t td_tex = ctx.terma.texture(0.0f, kAirDensity);
 
+    if (n > 0x7fffffffLL) throw Error(DC_ERR_VALUE, "photon volumes are limited to 2^31 - 1 voxels.");
     float *wet = static_cast<float *>(ctx.wet_raw.ensure((size_t)n * sizeof(float)));
     float *elec = static_cast<float *>(ctx.electron.ensure((size_t)n * sizeof(float)));
     float4 *dirs = static_cast<float4 *>(ctx.small.ensure(kMaxCones * 12 * sizeof(float4)));
+    char *act = static_cast<char *>(ctx.active.ensure(256 + (size_t)n * sizeof(int)));
+    unsigned *n_active = reinterpret_cast<unsigned *>(act);
+    int *active = reinterpret_cast<int *>(act + 256);
 
     launch_wet_march(ctx, g, f, dens_tex, wet, s);
+    DC_CUDA(cudaMemsetAsync(n_active, 0, sizeof(unsigned), s));
     {
         KernelTimer kt(ctx, "terma", s);
-        terma_kernel<<<vol_grid(g), dim3(32, 4, 1), 0, s>>>(g, f, P, wet, dens_tex, ctx.terma.surf, elec);
+        terma_kernel<<<vol_grid(g), dim3(32, 4, 1), 0, s>>>(g, f, P, wet, dens_tex, ctx.terma.surf, elec, dose_dev,
+                                                            active, n_active);
         check_launch("terma_kernel");
     }
     cone_dirs_kernel<<<1, kMaxCones * 12, 0, s>>>(f, C, dirs);
     check_launch("cone_dirs_kernel");
     {
+        // persistent grid: as many resident CTAs as fit on every SM
+        int sms = 0, per_sm = 0;
+        DC_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx.device));
+        DC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cccs_kernel, 128, 0));
+        const long long want = (n + 127) / 128;
+        const unsigned blocks = (unsigned)std::max(1LL, std::min<long long>(want, (long long)sms * std::max(per_sm, 1)));
         KernelTimer kt(ctx, "cccs", s);
-        cccs_kernel<<<vol_grid(g), dim3(32, 4, 1), 0, s>>>(g, f, C, g.sx / 10.0f, dose_scale, dirs, td_tex, elec,
-                                                           dose_dev);
+        cccs_kernel<<<blocks, 128, 0, s>>>(g, f, C, g.sx / 10.0f, dose_scale, dirs, td_tex, elec, active, n_active,
+                                           dose_dev);
         check_launch("cccs_kernel");
     }
 }

@@ -144,6 +144,7 @@ void DeviceContext::release_all() {
     vol_b.release();
     vol_c.release();
     electron.release();
+    active.release();
     small.release();
     lut.release();
     tables.release();

@@ -90,6 +90,7 @@ class DeviceContext {
     DeviceBuffer vol_b;       // generic volume scratch (output)
     DeviceBuffer vol_c;       // generic volume scratch (second output)
     DeviceBuffer electron;    // electron contamination term
+    DeviceBuffer active;      // CCCS active-voxel list (count in the first 256 B)
     DeviceBuffer small;       // per-call small device tables (cone directions)
     DeviceBuffer lut;         // proton LUT rows uploaded by the host entry point
     DeviceBuffer tables;      // proton layer + spot tables
