@@ -94,6 +94,19 @@ SIGNATURES = {
     "dc_proton_spot_dev": (C.c_int, _VOL + [_F3, C.c_double, C.c_float, C.c_float, C.c_float,
                                             C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
                                             C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
+    "dc_proton_beam_create": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, _F3, _F3, _F3, C.c_double, C.c_float,
+                                        C.c_float, C.c_float, C.c_void_p, C.c_int, C.c_int, C.c_void_p,
+                                        C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_int,
+                                        C.POINTER(C.c_void_p)]),
+    "dc_proton_beam_destroy": (C.c_int, [C.c_void_p]),
+    "dc_proton_beam_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                      C.POINTER(C.c_longlong)]),
+    "dc_proton_beam_dose": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "dc_proton_beam_adjoint": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "dc_proton_beam_influence_nnz": (C.c_int, [C.c_void_p, C.c_void_p, C.c_float, C.POINTER(C.c_longlong),
+                                               C.c_void_p]),
+    "dc_proton_beam_influence_csr": (C.c_int, [C.c_void_p, C.c_void_p, C.c_float, C.c_void_p, C.c_void_p,
+                                               C.c_void_p, C.c_longlong, C.c_void_p]),
     "dc_photon_dose": (C.c_int, _VOL + [C.POINTER(PhotonModel), C.POINTER(ControlPoint), C.c_void_p]),
     "dc_photon_dose_dev": (C.c_int, _VOL + [C.POINTER(PhotonModel), C.POINTER(ControlPoint), C.c_void_p,
                                             C.c_void_p]),

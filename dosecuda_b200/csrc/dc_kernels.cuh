@@ -28,8 +28,11 @@ struct LayerRec {
 
 // Spot record with the divergent-axis constants precomputed on the host:
 // t = (x/VSADX, y/VSADY, -1), inv_t2 = 1/|t|^2 (IMPTClasses.cu:123-133).
+// `orig` is the spot's row in the caller's spot list (records are sorted by
+// energy id).
 struct SpotRec {
-    float x, y, mu, pad0;
+    float x, y, mu;
+    int orig;
     float tx, ty, inv_t2, pad1;
 };
 
@@ -43,6 +46,23 @@ struct ProtonTables {
     int lut_len;
 };
 
+// Per-mode inputs/outputs of the pencil-beam kernel family (all device
+// pointers; spot-indexed arrays are in the caller's spot order).
+struct PbExtra {
+    const float *mu = nullptr;         // dose/adjoint: MU per spot (nullptr: the table's MU)
+    const float *grad_dose = nullptr;  // adjoint: dObjective/dDose per voxel
+    double *grad_mu = nullptr;         // adjoint: += sum_v grad_dose(v) * K_s(v)
+    unsigned *spot_max = nullptr;      // spot-max: max_v K_s(v) as float bits
+    const float *thr = nullptr;        // count/fill: keep K_s(v) >= thr[s]
+    int *counts = nullptr;             // count: entries per voxel row
+    const long long *row_ptr = nullptr;  // fill: CSR row starts (voxel rows)
+    int *col = nullptr;                // fill: spot index
+    float *val = nullptr;              // fill: dose per MU
+    long long cap = 0;                 // fill: capacity of col/val
+};
+
+enum PbMode { kPbDose = 0, kPbAdjoint = 1, kPbSpotMax = 2, kPbCount = 3, kPbFill = 4 };
+
 // Builds the sorted spot table and the layer table on the host.  Throws
 // Error(DC_ERR_VALUE) for malformed input.
 void build_proton_tables(const float *spots, int n_spots, const float *dvp, int n_energies, int dvp_len,
@@ -50,6 +70,10 @@ void build_proton_tables(const float *spots, int n_spots, const float *dvp, int 
                          std::vector<SpotRec> &spot_recs);
 
 void launch_pencil_beam(DeviceContext &ctx, const Grid &g, const Frame &f, const ProtonTables &t,
-                        const float *wet_s, float *dose, cudaStream_t s);
+                        const float *wet_s, float *dose, cudaStream_t s, const float *mu_dev = nullptr);
+
+// The other members of the family (see PbMode); `name` labels the profiler entry.
+void launch_pencil_beam_mode(DeviceContext &ctx, int mode, const Grid &g, const Frame &f, const ProtonTables &t,
+                             const float *wet_s, const PbExtra &x, cudaStream_t s);
 
 }  // namespace dc

@@ -76,7 +76,8 @@ void build_proton_tables(const float *spots, int n_spots, const float *dvp, int 
         o.tx = tmp[s].x / vsadx;
         o.ty = tmp[s].y / vsady;
         o.inv_t2 = 1.0f / (o.tx * o.tx + o.ty * o.ty + 1.0f);
-        o.pad0 = o.pad1 = 0.f;
+        o.orig = tmp[s].order;
+        o.pad1 = 0.f;
     }
     layers.clear();
     int s = 0;
@@ -145,30 +146,49 @@ __device__ __forceinline__ bool pb_voxel_layer(const LayerRec &L, const float *s
     return true;
 }
 
+// The pencil-beam kernel family.  Every member walks the same tiles, layers
+// and spots and evaluates the same per-pair influence
+//   K_s(v) = pf exp2(ps2 r^2) + hf exp2(hs2 r^2)   (dose per MU),
+// so the dose, its adjoint and the influence matrix agree to rounding.
+//   kPbDose     dose(v)       = sum_s mu_s K_s(v)          (one write per voxel)
+//   kPbAdjoint  grad_mu[s]   += sum_v g(v) K_s(v)          (warp reduction per spot,
+//                                                           one FP64 atomic per CTA and spot)
+//   kPbSpotMax  spot_max[s]   = max_v K_s(v)
+//   kPbCount    counts[v]     = #{s : K_s(v) >= thr[s]}
+//   kPbFill     CSR row v     = (s, K_s(v)) for K_s(v) >= thr[s], in spot-table order
+template <int kMode>
 __global__ void __launch_bounds__(kPbThreadsX *kPbThreadsY)
-    pencil_beam_kernel(Grid g, Frame f, ProtonTables t, const float *__restrict__ wet_s, float *__restrict__ dose) {
+    pb_kernel(Grid g, Frame f, ProtonTables t, const float *__restrict__ wet_s, float *__restrict__ dose, PbExtra x) {
     extern __shared__ float4 smem4[];
-    float4 *s_spot_a = smem4;                    // x, y, mu, -
-    float4 *s_spot_b = smem4 + kPbSpotChunk;     // tx, ty, inv_t2, -
-    float *s_lut = reinterpret_cast<float *>(smem4 + 2 * kPbSpotChunk);
+    float4 *s_spot_a = smem4;                    // x, y, mu, orig (int bits)
+    float4 *s_spot_b = smem4 + kPbSpotChunk;     // tx, ty, inv_t2, threshold
+    float *s_acc = reinterpret_cast<float *>(smem4 + 2 * kPbSpotChunk);  // adjoint partial sums
+    float *s_lut = s_acc + kPbSpotChunk;
     float *s_depth = s_lut;
     float *s_sigma = s_lut + t.lut_len;
     float *s_idd = s_lut + 2 * t.lut_len;
 
     const int tid = threadIdx.y * kPbThreadsX + threadIdx.x;
+    const int lane = threadIdx.x;
     const int nthreads = kPbThreadsX * kPbThreadsY;
     const int i = blockIdx.x * kPbThreadsX + threadIdx.x;
     const int j0 = blockIdx.y * (kPbThreadsY * kPbVoxY) + threadIdx.y;
     const int k = blockIdx.z;
 
     float hx[kPbVoxY], hy[kPbVoxY], hz[kPbVoxY], hz2[kPbVoxY], wet_mm[kPbVoxY], dsrc[kPbVoxY], acc[kPbVoxY];
+    float gv[kPbVoxY];
+    long long vidx[kPbVoxY];
+    long long fill_off[kPbVoxY], fill_end[kPbVoxY];
+    int cnt[kPbVoxY];
     bool inside[kPbVoxY];
 #pragma unroll
     for (int v = 0; v < kPbVoxY; ++v) {
         const int j = j0 + v * kPbThreadsY;
         inside[v] = (i < g.nx) && (j < g.ny);
         acc[v] = 0.0f;
+        cnt[v] = 0;
         const int ic = min(i, g.nx - 1), jc = min(j, g.ny - 1);
+        vidx[v] = (long long)ic + (long long)g.nx * (jc + (long long)g.ny * k);
         const float3 p = voxel_xyz(g, f, ic, jc, k);
         const float3 h = image_to_head<false>(f, p);
         hx[v] = h.x;
@@ -176,7 +196,14 @@ __global__ void __launch_bounds__(kPbThreadsX *kPbThreadsY)
         hz[v] = h.z;
         hz2[v] = h.z * h.z;
         dsrc[v] = distance_to_source(f, p);
-        wet_mm[v] = __ldg(wet_s + (long long)ic + (long long)g.nx * (jc + (long long)g.ny * k)) * 10.0f;
+        wet_mm[v] = __ldg(wet_s + vidx[v]) * 10.0f;
+        gv[v] = 0.0f;
+        if (kMode == kPbAdjoint) gv[v] = inside[v] ? __ldg(x.grad_dose + vidx[v]) : 0.0f;
+        fill_off[v] = fill_end[v] = 0;
+        if (kMode == kPbFill && inside[v]) {
+            fill_off[v] = x.row_ptr[vidx[v]];
+            fill_end[v] = min(x.row_ptr[vidx[v] + 1], x.cap);  // never past the counted row or the buffers
+        }
     }
 
     for (int l = 0; l < t.n_layers; ++l) {
@@ -212,60 +239,138 @@ __global__ void __launch_bounds__(kPbThreadsX *kPbThreadsY)
             if (c0 > 0) __syncthreads();
             const float4 *gsp = reinterpret_cast<const float4 *>(t.spots + L.spot_start + c0);
             for (int q = tid; q < cn; q += nthreads) {
-                s_spot_a[q] = __ldg(gsp + 2 * q);
-                s_spot_b[q] = __ldg(gsp + 2 * q + 1);
+                float4 a = __ldg(gsp + 2 * q);
+                float4 b = __ldg(gsp + 2 * q + 1);
+                const int orig = __float_as_int(a.w);
+                if (x.mu) a.z = __ldg(x.mu + orig);
+                if (kMode == kPbCount || kMode == kPbFill) b.w = __ldg(x.thr + orig);
+                s_spot_a[q] = a;
+                s_spot_b[q] = b;
+                if (kMode == kPbAdjoint) s_acc[q] = 0.0f;
             }
             __syncthreads();
-            if (!any) continue;
-            float accp[kPbVoxY], acch[kPbVoxY];
+            if (kMode == kPbDose) {
+                if (!any) continue;
+                float accp[kPbVoxY], acch[kPbVoxY];
 #pragma unroll
-            for (int v = 0; v < kPbVoxY; ++v) accp[v] = acch[v] = 0.f;
+                for (int v = 0; v < kPbVoxY; ++v) accp[v] = acch[v] = 0.f;
 #pragma unroll 4
-            for (int q = 0; q < cn; ++q) {
-                const float4 a = s_spot_a[q];
-                const float4 b = s_spot_b[q];
+                for (int q = 0; q < cn; ++q) {
+                    const float4 a = s_spot_a[q];
+                    const float4 b = s_spot_b[q];
+#pragma unroll
+                    for (int v = 0; v < kPbVoxY; ++v) {
+                        const float rx = hx[v] - a.x;
+                        const float ry = hy[v] - a.y;
+                        const float ray2 = fmaf(rx, rx, fmaf(ry, ry, hz2[v]));
+                        const float dot = fmaf(b.x, rx, fmaf(b.y, ry, -hz[v]));
+                        const float r2 = fmaf(-dot, dot * b.z, ray2);
+                        accp[v] = fmaf(a.z, fast_exp2(pv[v].ps2 * r2), accp[v]);
+                        acch[v] = fmaf(a.z, fast_exp2(pv[v].hs2 * r2), acch[v]);
+                    }
+                }
 #pragma unroll
                 for (int v = 0; v < kPbVoxY; ++v) {
-                    const float rx = hx[v] - a.x;
-                    const float ry = hy[v] - a.y;
-                    const float ray2 = fmaf(rx, rx, fmaf(ry, ry, hz2[v]));
-                    const float dot = fmaf(b.x, rx, fmaf(b.y, ry, -hz[v]));
-                    const float r2 = fmaf(-dot, dot * b.z, ray2);
-                    accp[v] = fmaf(a.z, fast_exp2(pv[v].ps2 * r2), accp[v]);
-                    acch[v] = fmaf(a.z, fast_exp2(pv[v].hs2 * r2), acch[v]);
+                    if (act[v]) acc[v] += fmaf(pv[v].pf, accp[v], pv[v].hf * acch[v]);
                 }
-            }
+            } else {
+                // modes that need the per-pair influence K_s(v)
+                for (int q = 0; q < cn; ++q) {
+                    const float4 a = s_spot_a[q];
+                    const float4 b = s_spot_b[q];
+                    float kv[kPbVoxY];
 #pragma unroll
-            for (int v = 0; v < kPbVoxY; ++v) {
-                if (act[v]) acc[v] += fmaf(pv[v].pf, accp[v], pv[v].hf * acch[v]);
+                    for (int v = 0; v < kPbVoxY; ++v) {
+                        const float rx = hx[v] - a.x;
+                        const float ry = hy[v] - a.y;
+                        const float ray2 = fmaf(rx, rx, fmaf(ry, ry, hz2[v]));
+                        const float dot = fmaf(b.x, rx, fmaf(b.y, ry, -hz[v]));
+                        const float r2 = fmaf(-dot, dot * b.z, ray2);
+                        kv[v] = act[v] ? fmaf(pv[v].pf, fast_exp2(pv[v].ps2 * r2), pv[v].hf * fast_exp2(pv[v].hs2 * r2))
+                                       : 0.0f;
+                    }
+                    if (kMode == kPbAdjoint) {
+                        float c = 0.0f;
+#pragma unroll
+                        for (int v = 0; v < kPbVoxY; ++v) c = fmaf(gv[v], kv[v], c);
+#pragma unroll
+                        for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+                        if (lane == 0 && c != 0.0f) atomicAdd(&s_acc[q], c);
+                    } else if (kMode == kPbSpotMax) {
+                        float m = fmaxf(kv[0], kv[1]);
+#pragma unroll
+                        for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+                        if (lane == 0 && m > 0.0f) atomicMax(x.spot_max + __float_as_int(a.w), __float_as_uint(m));
+                    } else if (kMode == kPbCount) {
+#pragma unroll
+                        for (int v = 0; v < kPbVoxY; ++v) cnt[v] += (act[v] && kv[v] >= b.w && kv[v] > 0.0f) ? 1 : 0;
+                    } else if (kMode == kPbFill) {
+#pragma unroll
+                        for (int v = 0; v < kPbVoxY; ++v) {
+                            if (act[v] && kv[v] >= b.w && kv[v] > 0.0f && fill_off[v] < fill_end[v]) {
+                                x.col[fill_off[v]] = __float_as_int(a.w);
+                                x.val[fill_off[v]] = kv[v];
+                                ++fill_off[v];
+                            }
+                        }
+                    }
+                }
+                if (kMode == kPbAdjoint) {
+                    __syncthreads();
+                    for (int q = tid; q < cn; q += nthreads) {
+                        const float c = s_acc[q];
+                        if (c != 0.0f) atomicAdd(x.grad_mu + __float_as_int(s_spot_a[q].w), (double)c);
+                    }
+                }
             }
         }
     }
 
 #pragma unroll
     for (int v = 0; v < kPbVoxY; ++v) {
-        const int j = j0 + v * kPbThreadsY;
-        if (inside[v]) dose[(long long)i + (long long)g.nx * (j + (long long)g.ny * k)] = acc[v];
+        if (!inside[v]) continue;
+        if (kMode == kPbDose) dose[vidx[v]] = acc[v];
+        if (kMode == kPbCount) x.counts[vidx[v]] = cnt[v];
     }
 }
 
-void launch_pencil_beam(DeviceContext &ctx, const Grid &g, const Frame &f, const ProtonTables &t,
-                        const float *wet_s, float *dose, cudaStream_t s) {
-    const size_t smem = 2 * kPbSpotChunk * sizeof(float4) + 3 * (size_t)t.lut_len * sizeof(float);
+static size_t pb_smem(const ProtonTables &t) {
+    return 2 * kPbSpotChunk * sizeof(float4) + kPbSpotChunk * sizeof(float) + 3 * (size_t)t.lut_len * sizeof(float);
+}
+
+template <int kMode>
+static void pb_launch(DeviceContext &ctx, const char *name, const Grid &g, const Frame &f, const ProtonTables &t,
+                      const float *wet_s, float *dose, const PbExtra &x, cudaStream_t s) {
+    const size_t smem = pb_smem(t);
     static bool attr_set[64] = {false};
-    if (smem > 48 * 1024) {
-        if (ctx.device < 64 && !attr_set[ctx.device]) {
-            DC_CUDA(cudaFuncSetAttribute(pencil_beam_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         200 * 1024));
-            attr_set[ctx.device] = true;
-        }
+    if (smem > 48 * 1024 && ctx.device < 64 && !attr_set[ctx.device]) {
+        DC_CUDA(cudaFuncSetAttribute(pb_kernel<kMode>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+        attr_set[ctx.device] = true;
     }
     dim3 block(kPbThreadsX, kPbThreadsY, 1);
     dim3 grid((unsigned)((g.nx + kPbThreadsX - 1) / kPbThreadsX),
               (unsigned)((g.ny + kPbThreadsY * kPbVoxY - 1) / (kPbThreadsY * kPbVoxY)), (unsigned)g.nz);
-    KernelTimer kt(ctx, "pencil_beam", s);
-    pencil_beam_kernel<<<grid, block, smem, s>>>(g, f, t, wet_s, dose);
-    check_launch("pencil_beam_kernel");
+    KernelTimer kt(ctx, name, s);
+    pb_kernel<kMode><<<grid, block, smem, s>>>(g, f, t, wet_s, dose, x);
+    check_launch(name);
+}
+
+void launch_pencil_beam(DeviceContext &ctx, const Grid &g, const Frame &f, const ProtonTables &t,
+                        const float *wet_s, float *dose, cudaStream_t s, const float *mu_dev) {
+    PbExtra x;
+    x.mu = mu_dev;
+    pb_launch<kPbDose>(ctx, "pencil_beam", g, f, t, wet_s, dose, x, s);
+}
+
+void launch_pencil_beam_mode(DeviceContext &ctx, int mode, const Grid &g, const Frame &f, const ProtonTables &t,
+                             const float *wet_s, const PbExtra &x, cudaStream_t s) {
+    switch (mode) {
+        case kPbAdjoint: pb_launch<kPbAdjoint>(ctx, "pencil_beam_adjoint", g, f, t, wet_s, nullptr, x, s); break;
+        case kPbSpotMax: pb_launch<kPbSpotMax>(ctx, "pencil_beam_spotmax", g, f, t, wet_s, nullptr, x, s); break;
+        case kPbCount: pb_launch<kPbCount>(ctx, "pencil_beam_count", g, f, t, wet_s, nullptr, x, s); break;
+        case kPbFill: pb_launch<kPbFill>(ctx, "pencil_beam_fill", g, f, t, wet_s, nullptr, x, s); break;
+        default: throw Error(DC_ERR_VALUE, "unknown pencil-beam mode");
+    }
 }
 
 }  // namespace dc

@@ -117,3 +117,133 @@ def profile(gpu_id: int = 0, enable: bool | None = None, reset: bool = False):
     if reset:
         _lib.raise_for(lib.dc_profile_reset(gpu_id))
     return _lib.profile_read(gpu_id)
+
+
+class ProtonBeamPlan:
+    """One proton beam resident on a device, for plan optimisation.
+
+    Holds the sorted spot and layer tables and the depth-dose tables on the
+    GPU (C ABI ``dc_proton_beam_*``).  Given the beam's smoothed WET it gives
+    the dose for any spot weights, the adjoint D^T g of a dose gradient, and the
+    dose-influence matrix in CSR.  Spot-indexed tensors follow the order of
+    ``beam.spot_list``."""
+
+    def __init__(self, grid, beam, model, device="cuda", spots=None):
+        dev = torch.device(device)
+        if dev.index is None:
+            dev = torch.device("cuda", torch.cuda.current_device())
+        self.device = dev
+        sp = np.ascontiguousarray(beam.spot_list if spots is None else spots, dtype=np.float32).reshape(-1, 4)
+        self.n_spots = sp.shape[0]
+        dvp = np.ascontiguousarray(model.divergence_params, dtype=np.float32)
+        ld, ls, li = (np.ascontiguousarray(a, dtype=np.float32) for a in (model.lut_depths, model.lut_sigmas,
+                                                                          model.lut_idds))
+        self._mu0 = torch.as_tensor(sp[:, 2].copy(), device=dev)
+        self._grid, self._beam, self._model = grid, beam, model
+        self._h = C.c_void_p()
+        self._sp, self._dvp, self._luts = sp, dvp, (ld, ls, li)
+        self._created_for = None
+
+    def _handle(self, shape):
+        if self._created_for == shape:
+            return self._h
+        self.close()
+        lib = _lib.load()
+        nz, ny, nx = shape
+        ld, ls, li = self._luts
+        h = C.c_void_p()
+        with torch.cuda.device(self.device):
+            rc = lib.dc_proton_beam_create(
+                self.device.index, nz, ny, nx, _spacing(self._grid), _lib.f3(self._grid.origin),
+                _lib.f3(self._beam.iso), float(self._beam.gantry_angle), float(self._beam.couch_angle),
+                float(self._model.VSADX), float(self._model.VSADY), self._dvp.ctypes.data_as(C.c_void_p),
+                ld.shape[0], self._dvp.shape[1], ld.ctypes.data_as(C.c_void_p), ls.ctypes.data_as(C.c_void_p),
+                li.ctypes.data_as(C.c_void_p), ld.shape[1], self._sp.ctypes.data_as(C.c_void_p), self.n_spots,
+                C.byref(h))
+        _lib.raise_for(rc)
+        self._h, self._created_for = h, shape
+        return h
+
+    def close(self):
+        if self._h:
+            _lib.load().dc_proton_beam_destroy(self._h)
+            self._h = C.c_void_p()
+            self._created_for = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def mu(self) -> torch.Tensor:
+        """The MU column of the spot list, on the device."""
+        return self._mu0
+
+    def dose(self, wet: torch.Tensor, mu: torch.Tensor | None = None, out=None, stream=None) -> torch.Tensor:
+        _check_volume(wet, "wet")
+        h = self._handle(tuple(wet.shape))
+        out = _out(wet, out)
+        mu_p = None
+        if mu is not None:
+            mu = mu.detach().to(device=wet.device, dtype=torch.float32).contiguous()
+            if mu.numel() != self.n_spots:
+                raise ValueError("mu must hold one weight per spot")
+            mu_p = C.c_void_p(mu.data_ptr())
+        rc = _lib.load().dc_proton_beam_dose(h, C.c_void_p(wet.data_ptr()), mu_p, C.c_void_p(out.data_ptr()),
+                                             _stream(wet, stream))
+        _lib.raise_for(rc)
+        return out
+
+    def adjoint(self, wet: torch.Tensor, grad_dose: torch.Tensor, stream=None) -> torch.Tensor:
+        """D^T g: float64 tensor with one entry per spot."""
+        _check_volume(wet, "wet")
+        g = grad_dose.detach().to(device=wet.device, dtype=torch.float32).contiguous()
+        if g.shape != wet.shape:
+            raise ValueError("grad_dose must have the volume's shape")
+        h = self._handle(tuple(wet.shape))
+        out = torch.empty(self.n_spots, dtype=torch.float64, device=wet.device)
+        rc = _lib.load().dc_proton_beam_adjoint(h, C.c_void_p(wet.data_ptr()), C.c_void_p(g.data_ptr()),
+                                                C.c_void_p(out.data_ptr()), _stream(wet, stream))
+        _lib.raise_for(rc)
+        return out
+
+    def influence_csr(self, wet: torch.Tensor, cutoff: float = 1e-4, stream=None):
+        """(row_ptr int64[n_voxels+1], col int32[nnz], val float32[nnz]) of the
+        voxels x spots influence matrix, entries >= cutoff x the spot's maximum."""
+        _check_volume(wet, "wet")
+        h = self._handle(tuple(wet.shape))
+        lib = _lib.load()
+        nnz = C.c_longlong(0)
+        _lib.raise_for(lib.dc_proton_beam_influence_nnz(h, C.c_void_p(wet.data_ptr()), float(cutoff),
+                                                        C.byref(nnz), _stream(wet, stream)))
+        n_vox = wet.numel()
+        row_ptr = torch.empty(n_vox + 1, dtype=torch.int64, device=wet.device)
+        col = torch.empty(max(nnz.value, 1), dtype=torch.int32, device=wet.device)
+        val = torch.empty(max(nnz.value, 1), dtype=torch.float32, device=wet.device)
+        _lib.raise_for(lib.dc_proton_beam_influence_csr(h, C.c_void_p(wet.data_ptr()), float(cutoff),
+                                                        C.c_void_p(row_ptr.data_ptr()), C.c_void_p(col.data_ptr()),
+                                                        C.c_void_p(val.data_ptr()), nnz.value, _stream(wet, stream)))
+        return row_ptr, col[:nnz.value], val[:nnz.value]
+
+
+class _ProtonDoseFn(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, mu, wet, plan):
+        ctx.plan = plan
+        ctx.save_for_backward(wet)
+        ctx.mu_dtype = mu.dtype
+        return plan.dose(wet, mu)
+
+    @staticmethod
+    def backward(ctx, grad_dose):
+        (wet,) = ctx.saved_tensors
+        g = ctx.plan.adjoint(wet, grad_dose)
+        return g.to(ctx.mu_dtype), None, None
+
+
+def proton_dose_autograd(mu: torch.Tensor, wet: torch.Tensor, plan: ProtonBeamPlan) -> torch.Tensor:
+    """Differentiable dose of one beam in its spot weights: forward is the
+    pencil-beam kernel, backward the hand-written adjoint kernel (D^T g)."""
+    return _ProtonDoseFn.apply(mu, wet, plan)

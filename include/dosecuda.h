@@ -194,6 +194,50 @@ int dc_proton_spot_dev(int gpu_id,
                        float *dose_out_dev, void *stream);
 
 /* ------------------------------------------------------------------ */
+/* Proton beam kept on the device: dose from device-side spot weights,  */
+/* the adjoint D^T g and the dose-influence matrix.  No counterpart in  */
+/* the reference beyond its WET reuse (computeIMPTWET /                 */
+/* computeIMPTPlanFromWET, plan_impt.py:162-211).  The handle holds the */
+/* sorted spot/layer tables and the LUTs on its device; every call uses */
+/* the same per-pair influence K_s(v) (dose per MU of spot s in voxel v)*/
+/* as dc_proton_spot.  Spot-indexed arrays are in the order of `spots`. */
+/* ------------------------------------------------------------------ */
+typedef struct dc_proton_beam dc_proton_beam;
+
+/* Arguments as dc_proton_spot, all host arrays (copied to the device). */
+int dc_proton_beam_create(int gpu_id, int nz, int ny, int nx,
+                          const float spacing[3], const float origin[3],
+                          const float iso[3], double gantry_deg, float couch_deg,
+                          float vsadx, float vsady,
+                          const float *divergence_params, int n_energies, int dvp_len,
+                          const float *lut_depths, const float *lut_sigmas,
+                          const float *lut_idds, int lut_len,
+                          const float *spots, int n_spots,
+                          dc_proton_beam **out);
+int dc_proton_beam_destroy(dc_proton_beam *beam);
+int dc_proton_beam_info(const dc_proton_beam *beam, int *n_spots, int *n_layers, long long *n_voxels);
+
+/* dose_dev[v] = sum_s mu_s K_s(v); mu_dev: n_spots floats on the device, or
+ * NULL for the MU column of the spot list. */
+int dc_proton_beam_dose(dc_proton_beam *beam, const float *wet_dev, const float *mu_dev,
+                        float *dose_dev, void *stream);
+
+/* grad_mu_dev[s] = sum_v grad_dose_dev[v] K_s(v) (FP64, overwritten). */
+int dc_proton_beam_adjoint(dc_proton_beam *beam, const float *wet_dev, const float *grad_dose_dev,
+                           double *grad_mu_dev, void *stream);
+
+/* Influence matrix A (voxels x spots) in CSR with voxel rows: entries
+ * K_s(v) >= cutoff * max_v K_s(v).  _nnz computes the entry count
+ * (synchronises); _csr fills row_ptr_dev (n_voxels + 1, int64), col_dev
+ * (spot index, int32) and val_dev (float32), writing at most `capacity`
+ * entries. */
+int dc_proton_beam_influence_nnz(dc_proton_beam *beam, const float *wet_dev, float cutoff,
+                                 long long *nnz, void *stream);
+int dc_proton_beam_influence_csr(dc_proton_beam *beam, const float *wet_dev, float cutoff,
+                                 long long *row_ptr_dev, int *col_dev, float *val_dev,
+                                 long long capacity, void *stream);
+
+/* ------------------------------------------------------------------ */
 /* Photon: ray trace + TERMA + collapsed-cone convolution/superposition */
 /* Replaces dose_kernels.photon_dose_cuda                               */
 /* (dosemodule.cu:377-557 -> IMRTClasses.cu:353-405).                   */
