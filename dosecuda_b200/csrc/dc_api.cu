@@ -85,14 +85,17 @@ void proton_spot_core(DeviceContext &ctx, const Grid &g, const Frame &f, const s
     const size_t lb = layers.size() * sizeof(LayerRec);
     const size_t lb_al = (lb + 255) & ~(size_t)255;
     const size_t sb = spots.size() * sizeof(SpotRec);
-    char *pin = static_cast<char *>(ctx.pin_small.ensure(lb_al + sb));
-    // The previous call's copy out of the staging buffer must be done.
-    DC_CUDA(cudaEventSynchronize(ctx.pin_free));
+    const int slot = ctx.pin_next;
+    ctx.pin_next = (ctx.pin_next + 1) % DeviceContext::kPinSlots;
+    // The copy that last used this staging slot must be done before it is rewritten.
+    DC_CUDA(cudaEventSynchronize(ctx.pin_ev[slot]));
+    char *pin = static_cast<char *>(ctx.pin_ring[slot].ensure(lb_al + sb));
     std::memcpy(pin, layers.data(), lb);
     std::memcpy(pin + lb_al, spots.data(), sb);
     char *dev = static_cast<char *>(ctx.tables.ensure(lb_al + sb));
     DC_CUDA(cudaMemcpyAsync(dev, pin, lb_al + sb, cudaMemcpyHostToDevice, s));
-    DC_CUDA(cudaEventRecord(ctx.pin_free, s));
+    DC_CUDA(cudaEventRecord(ctx.pin_ev[slot], s));
+    launch_layer_rcut(g, f, reinterpret_cast<LayerRec *>(dev), (int)layers.size(), lut_d, lut_s, lut_len, s);
     ProtonTables t;
     t.layers = reinterpret_cast<const LayerRec *>(dev);
     t.spots = reinterpret_cast<const SpotRec *>(dev + lb_al);

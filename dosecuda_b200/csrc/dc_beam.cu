@@ -230,6 +230,9 @@ int dc_proton_beam_create(int gpu_id, int nz, int ny, int nx, const float spacin
         DC_CUDA(cudaMemcpy(lp, lut_depths, lbytes, cudaMemcpyHostToDevice));
         DC_CUDA(cudaMemcpy(lp + b->lut_stride, lut_sigmas, lbytes, cudaMemcpyHostToDevice));
         DC_CUDA(cudaMemcpy(lp + 2 * b->lut_stride, lut_idds, lbytes, cudaMemcpyHostToDevice));
+        launch_layer_rcut(b->g, b->f, static_cast<LayerRec *>(tp), b->n_layers, reinterpret_cast<const float *>(lp),
+                          reinterpret_cast<const float *>(lp + b->lut_stride), lut_len, nullptr);
+        DC_CUDA(cudaDeviceSynchronize());
         *out = b.release();
     });
 }

@@ -23,8 +23,12 @@ struct LayerRec {
     int energy_id;
     float r80;
     float A, B, C;  // sigma_air quadratic coefficients (divergence_params[2..4])
-    float pad;
+    float rcut;     // lateral cut-off radius (mm): 6 x the widest halo sigma of the layer
 };
+
+// Fills LayerRec::rcut on the device from the LUT rows (layer_rcut_kernel).
+void launch_layer_rcut(const Grid &g, const Frame &f, LayerRec *layers, int n_layers, const float *lut_depths,
+                       const float *lut_sigmas, int lut_len, cudaStream_t s);
 
 // Spot record with the divergent-axis constants precomputed on the host:
 // t = (x/VSADX, y/VSADY, -1), inv_t2 = 1/|t|^2 (IMPTClasses.cu:123-133).

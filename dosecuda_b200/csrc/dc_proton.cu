@@ -40,6 +40,7 @@ constexpr int kPbThreadsX = 32;
 constexpr int kPbThreadsY = 8;
 constexpr int kPbVoxY = 2;      // voxels per thread along y
 constexpr int kPbSpotChunk = 512;
+static_assert(2 * kPbThreadsX * kPbThreadsY == kPbSpotChunk, "two spots per thread per staging round");
 
 void build_proton_tables(const float *spots, int n_spots, const float *dvp, int n_energies, int dvp_len,
                          float vsadx, float vsady, std::vector<LayerRec> &layers,
@@ -94,7 +95,7 @@ void build_proton_tables(const float *spots, int n_spots, const float *dvp, int 
         L.A = row[2];
         L.B = row[3];
         L.C = row[4];
-        L.pad = 0.f;
+        L.rcut = INFINITY;  // set on the device by layer_rcut_kernel
         layers.push_back(L);
         s = t;
     }
@@ -144,6 +145,63 @@ __device__ __forceinline__ bool pb_voxel_layer(const LayerRec &L, const float *s
     o.ps2 = (sigma_t != 0.0f ? -0.5f / sqr(sigma_t) : -INFINITY) * kLog2e;
     o.hs2 = (sigma_ht != 0.0f ? -0.5f / sqr(sigma_ht) : -INFINITY) * kLog2e;
     return true;
+}
+
+// Lateral cut-off per layer.  A spot's Gaussians are negligible beyond
+// 6 sigma_ht (exp(-18) = 1.5e-8 of the halo peak); sigma_ht = hypot(sigma_t,
+// sigma_h) is bounded over every voxel the layer can reach:
+//  * |sigma_mcs| by the largest LUT sigma at depths up to 1.1 R80 (linear
+//    interpolation stays between table entries);
+//  * |sigma_air| by the quadratic's extremes over the range of
+//    d = |voxel - source| - w + 0.7 R80 for voxels of the volume;
+//  * sigma_h by sampling the halo formula over [0.1, R80 - 0.1] mm.
+__global__ void layer_rcut_kernel(Grid g, Frame f, LayerRec *layers, int n_layers, const float *lut_depths,
+                                  const float *lut_sigmas, int lut_len) {
+    const int l = blockIdx.x * blockDim.x + threadIdx.x;
+    if (l >= n_layers) return;
+    LayerRec &L = layers[l];
+    // source distance range over the volume's bounding box (image frame, relative to iso)
+    const float lo[3] = {-f.isox - 0.5f * g.sx, -f.isoy - 0.5f * g.sy, -f.isoz - 0.5f * g.sz};
+    const float hi[3] = {(g.nx - 0.5f) * g.sx - f.isox, (g.ny - 0.5f) * g.sy - f.isoy, (g.nz - 0.5f) * g.sz - f.isoz};
+    const float src[3] = {f.srcx, f.srcy, f.srcz};
+    float dmin2 = 0.f, dmax2 = 0.f;
+    for (int a = 0; a < 3; ++a) {
+        const float c = fminf(fmaxf(src[a], lo[a]), hi[a]);
+        dmin2 += sqr(src[a] - c);
+        dmax2 += fmaxf(sqr(src[a] - lo[a]), sqr(src[a] - hi[a]));
+    }
+    const float r80 = L.r80;
+    const float wmax = 1.1f * r80;
+    const float *D = lut_depths + (size_t)L.energy_id * lut_len;
+    const float *S = lut_sigmas + (size_t)L.energy_id * lut_len;
+    float smcs = 0.f;
+    for (int q = 0; q < lut_len; ++q) {
+        smcs = fmaxf(smcs, fabsf(S[q]));
+        if (D[q] > wmax) break;  // the row bracketing wmax from above is included
+    }
+    const float d0 = sqrtf(dmin2) - wmax + 0.7f * r80 - 1.0f;
+    const float d1 = sqrtf(dmax2) + 0.5f + 0.7f * r80 + 1.0f;
+    auto sair = [&](float d) { return fabsf(fmaf(fmaf(L.A, d, L.B), d, L.C)); };
+    float sa = fmaxf(sair(d0), sair(d1));
+    if (L.A != 0.0f) {
+        const float dv = -L.B / (2.0f * L.A);
+        if (dv > d0 && dv < d1) sa = fmaxf(sa, sair(dv));
+    }
+    float sh = 0.f;
+    for (float w = 0.1f; w <= r80 - 0.1f; w += 0.25f) {
+        const float h = 2.85f + (0.0014f * r80 * logf(w + 3.0f)) + (0.06f * w) - (7.4e-5f * sqr(w)) -
+                        ((0.22f * r80) / sqr(w - r80 - 5.0f));
+        sh = fmaxf(sh, h);
+    }
+    const float sht = hypotf(sa + smcs, sh * 1.02f + 0.2f) * 1.01f + 0.5f;
+    L.rcut = (sht == sht) ? 6.0f * sht : INFINITY;
+}
+
+void launch_layer_rcut(const Grid &g, const Frame &f, LayerRec *layers, int n_layers, const float *lut_depths,
+                       const float *lut_sigmas, int lut_len, cudaStream_t s) {
+    if (n_layers <= 0) return;
+    layer_rcut_kernel<<<(n_layers + 63) / 64, 64, 0, s>>>(g, f, layers, n_layers, lut_depths, lut_sigmas, lut_len);
+    check_launch("layer_rcut_kernel");
 }
 
 // The pencil-beam kernel family.  Every member walks the same tiles, layers
@@ -206,6 +264,44 @@ __global__ void __launch_bounds__(kPbThreadsX *kPbThreadsY)
         }
     }
 
+    // Beam's-eye-view bounding box of the CTA's voxels (for spot culling).
+    __shared__ float s_red[kPbThreadsY][6];
+    __shared__ float s_bb[6];
+    __shared__ int s_wcnt[kPbThreadsY];
+    {
+        float b[6] = {INFINITY, -INFINITY, INFINITY, -INFINITY, INFINITY, -INFINITY};
+#pragma unroll
+        for (int v = 0; v < kPbVoxY; ++v) {
+            if (!inside[v]) continue;
+            b[0] = fminf(b[0], hx[v]);
+            b[1] = fmaxf(b[1], hx[v]);
+            b[2] = fminf(b[2], hy[v]);
+            b[3] = fmaxf(b[3], hy[v]);
+            b[4] = fminf(b[4], hz[v]);
+            b[5] = fmaxf(b[5], hz[v]);
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+#pragma unroll
+            for (int c = 0; c < 6; c += 2) {
+                b[c] = fminf(b[c], __shfl_xor_sync(0xffffffffu, b[c], o));
+                b[c + 1] = fmaxf(b[c + 1], __shfl_xor_sync(0xffffffffu, b[c + 1], o));
+            }
+        }
+        if (lane == 0) {
+#pragma unroll
+            for (int c = 0; c < 6; ++c) s_red[threadIdx.y][c] = b[c];
+        }
+        __syncthreads();
+        if (tid < 6) {
+            float r = s_red[0][tid];
+            for (int w = 1; w < kPbThreadsY; ++w) r = (tid & 1) ? fmaxf(r, s_red[w][tid]) : fminf(r, s_red[w][tid]);
+            s_bb[tid] = r;
+        }
+        __syncthreads();
+    }
+    const float bx0 = s_bb[0], bx1 = s_bb[1], by0 = s_bb[2], by1 = s_bb[3], bz0 = s_bb[4], bz1 = s_bb[5];
+
     for (int l = 0; l < t.n_layers; ++l) {
         const LayerRec L = t.layers[l];
         __syncthreads();  // previous layer's shared data no longer in use
@@ -234,21 +330,62 @@ __global__ void __launch_bounds__(kPbThreadsX *kPbThreadsY)
         const bool block_any = __syncthreads_or(any);
         if (!block_any) continue;
 
+        const float rcut2 = L.rcut * L.rcut;
         for (int c0 = 0; c0 < L.n_spots; c0 += kPbSpotChunk) {
-            const int cn = min(kPbSpotChunk, L.n_spots - c0);
+            const int craw = min(kPbSpotChunk, L.n_spots - c0);
             if (c0 > 0) __syncthreads();
+            // Each thread tests two consecutive spots; the ones whose divergent
+            // axis comes within rcut of the CTA's box are compacted in order.
             const float4 *gsp = reinterpret_cast<const float4 *>(t.spots + L.spot_start + c0);
-            for (int q = tid; q < cn; q += nthreads) {
-                float4 a = __ldg(gsp + 2 * q);
-                float4 b = __ldg(gsp + 2 * q + 1);
+            float4 a2[2], b2[2];
+            bool keep[2];
+#pragma unroll
+            for (int u = 0; u < 2; ++u) {
+                const int q = 2 * tid + u;
+                keep[u] = false;
+                if (q < craw) {
+                    a2[u] = __ldg(gsp + 2 * q);
+                    b2[u] = __ldg(gsp + 2 * q + 1);
+                    // axis position at the box's height range: x(hz) = sx - tx * hz
+                    const float ax0 = a2[u].x - b2[u].x * bz0, ax1 = a2[u].x - b2[u].x * bz1;
+                    const float ay0 = a2[u].y - b2[u].y * bz0, ay1 = a2[u].y - b2[u].y * bz1;
+                    const float dx = fmaxf(0.0f, fmaxf(fminf(ax0, ax1) - bx1, bx0 - fmaxf(ax0, ax1)));
+                    const float dy = fmaxf(0.0f, fmaxf(fminf(ay0, ay1) - by1, by0 - fmaxf(ay0, ay1)));
+                    // perpendicular distance >= lateral distance * cos(tilt), cos^2 = inv_t2
+                    keep[u] = !((dx * dx + dy * dy) * b2[u].z > rcut2);
+                }
+            }
+            const int mine = (int)keep[0] + (int)keep[1];
+            int incl = mine;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int n = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += n;
+            }
+            if (lane == 31) s_wcnt[threadIdx.y] = incl;
+            __syncthreads();
+            int base = 0, cn = 0;
+#pragma unroll
+            for (int w = 0; w < kPbThreadsY; ++w) {
+                const int c = s_wcnt[w];
+                base += (w < (int)threadIdx.y) ? c : 0;
+                cn += c;
+            }
+            int pos = base + incl - mine;
+#pragma unroll
+            for (int u = 0; u < 2; ++u) {
+                if (!keep[u]) continue;
+                float4 a = a2[u], b = b2[u];
                 const int orig = __float_as_int(a.w);
                 if (x.mu) a.z = __ldg(x.mu + orig);
                 if (kMode == kPbCount || kMode == kPbFill) b.w = __ldg(x.thr + orig);
-                s_spot_a[q] = a;
-                s_spot_b[q] = b;
-                if (kMode == kPbAdjoint) s_acc[q] = 0.0f;
+                s_spot_a[pos] = a;
+                s_spot_b[pos] = b;
+                if (kMode == kPbAdjoint) s_acc[pos] = 0.0f;
+                ++pos;
             }
             __syncthreads();
+            if (cn == 0) continue;
             if (kMode == kPbDose) {
                 if (!any) continue;
                 float accp[kPbVoxY], acch[kPbVoxY];

@@ -126,13 +126,23 @@ void VolumeArray::release() {
 DeviceContext::DeviceContext(int dev) : device(dev) {
     DC_CUDA(cudaSetDevice(dev));
     DC_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
-    DC_CUDA(cudaEventCreateWithFlags(&pin_free, cudaEventDisableTiming));
+    for (auto &e : pin_ev) DC_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     DC_CUDA(cudaEventCreateWithFlags(&last_use, cudaEventDisableTiming));
 }
 
-void DeviceContext::begin_call(cudaStream_t s) { DC_CUDA(cudaStreamWaitEvent(s, last_use, 0)); }
+bool DeviceContext::capturing(cudaStream_t s) {
+    cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
+    DC_CUDA(cudaStreamIsCapturing(s, &st));
+    return st != cudaStreamCaptureStatusNone;
+}
 
-void DeviceContext::end_call(cudaStream_t s) { DC_CUDA(cudaEventRecord(last_use, s)); }
+void DeviceContext::begin_call(cudaStream_t s) {
+    if (!capturing(s)) DC_CUDA(cudaStreamWaitEvent(s, last_use, 0));
+}
+
+void DeviceContext::end_call(cudaStream_t s) {
+    if (!capturing(s)) DC_CUDA(cudaEventRecord(last_use, s));
+}
 
 DeviceContext::~DeviceContext() { release_all(); }
 
@@ -150,7 +160,7 @@ void DeviceContext::release_all() {
     tables.release();
     density.release();
     terma.release();
-    pin_small.release();
+    for (auto &b : pin_ring) b.release();
     for (auto &p : pending) {
         event_pool.push_back(p.a);
         event_pool.push_back(p.b);
@@ -158,9 +168,12 @@ void DeviceContext::release_all() {
     pending.clear();
     for (auto e : event_pool) cudaEventDestroy(e);
     event_pool.clear();
-    if (pin_free) cudaEventDestroy(pin_free);
+    for (auto &e : pin_ev) {
+        if (e) cudaEventDestroy(e);
+        e = nullptr;
+    }
     if (last_use) cudaEventDestroy(last_use);
-    pin_free = last_use = nullptr;
+    last_use = nullptr;
     if (stream) cudaStreamDestroy(stream);
     stream = nullptr;
 }

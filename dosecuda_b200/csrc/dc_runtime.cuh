@@ -96,14 +96,21 @@ class DeviceContext {
     DeviceBuffer tables;      // proton layer + spot tables
     VolumeArray density;      // density / RLSP texture
     VolumeArray terma;        // TERMA texture (surface-writable)
-    PinnedBuffer pin_small;   // staging for per-call tables
-    cudaEvent_t pin_free = nullptr;  // recorded after the last copy out of pin_small
+    // Ring of pinned staging slots for per-call tables: the host reuses a slot
+    // only after the copy out of it (event) has completed.
+    static constexpr int kPinSlots = 4;
+    PinnedBuffer pin_ring[kPinSlots];
+    cudaEvent_t pin_ev[kPinSlots] = {};
+    int pin_next = 0;
     cudaEvent_t last_use = nullptr;  // recorded after the last enqueued call
 
     // Orders a call on stream s after every earlier call on this device
-    // (the cached scratch buffers are shared), and marks its end.
+    // (the cached scratch buffers are shared), and marks its end.  While s is
+    // being captured into a CUDA graph the graph's own edges order the work,
+    // so neither the wait nor the record is issued (nor profiler events).
     void begin_call(cudaStream_t s);
     void end_call(cudaStream_t s);
+    static bool capturing(cudaStream_t s);
 
     // Profiler.
     bool profiling = false;
@@ -124,7 +131,8 @@ class DeviceContext {
 };
 
 // Returns the context for `device` (created on first use) with the device
-// made current.  Throws Error(DC_ERR_VALUE) for an invalid ordinal.
+// made current.  Throws Error(DC_ERR_CUDA) for an invalid ordinal, as the
+// reference's cudaSetDevice failure surfaces as a CUDA error.
 DeviceContext &context(int device);
 void release_context(int device);
 
@@ -134,7 +142,7 @@ struct KernelTimer {
     cudaStream_t s;
     cudaEvent_t a = nullptr, b = nullptr;
     KernelTimer(DeviceContext &c, const char *name, cudaStream_t st) : ctx(c), s(st) {
-        if (ctx.profiling) ctx.prof_begin(name, s, &a, &b);
+        if (ctx.profiling && !DeviceContext::capturing(s)) ctx.prof_begin(name, s, &a, &b);
     }
     ~KernelTimer() {
         if (b) ctx.prof_end(b, s);
