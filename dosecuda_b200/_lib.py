@@ -107,6 +107,19 @@ SIGNATURES = {
                                                C.c_void_p]),
     "dc_proton_beam_influence_csr": (C.c_int, [C.c_void_p, C.c_void_p, C.c_float, C.c_void_p, C.c_void_p,
                                                C.c_void_p, C.c_longlong, C.c_void_p]),
+    "dc_proton_batch_create": (C.c_int, [C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p,
+                                         C.c_void_p, C.c_int, C.c_float, C.c_float, C.POINTER(C.c_void_p)]),
+    "dc_proton_batch_add_plan": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, _F3, _F3, C.c_void_p,
+                                           C.c_void_p, C.POINTER(C.c_int)]),
+    "dc_proton_batch_add_beam": (C.c_int, [C.c_void_p, C.c_int, _F3, C.c_double, C.c_float, C.c_void_p, C.c_int,
+                                           C.c_void_p, C.POINTER(C.c_int)]),
+    "dc_proton_batch_commit": (C.c_int, [C.c_void_p]),
+    "dc_proton_batch_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                       C.POINTER(C.c_int)]),
+    "dc_proton_batch_beam_spot_offset": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int)]),
+    "dc_proton_batch_wet": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "dc_proton_batch_dose": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]),
+    "dc_proton_batch_destroy": (C.c_int, [C.c_void_p]),
     "dc_photon_dose": (C.c_int, _VOL + [C.POINTER(PhotonModel), C.POINTER(ControlPoint), C.c_void_p]),
     "dc_photon_dose_dev": (C.c_int, _VOL + [C.POINTER(PhotonModel), C.POINTER(ControlPoint), C.c_void_p,
                                             C.c_void_p]),

@@ -80,4 +80,25 @@ void launch_pencil_beam(DeviceContext &ctx, const Grid &g, const Frame &f, const
 void launch_pencil_beam_mode(DeviceContext &ctx, int mode, const Grid &g, const Frame &f, const ProtonTables &t,
                              const float *wet_s, const PbExtra &x, cudaStream_t s);
 
+// ---- batched pencil beam (persistent, many plans) -------------------------
+struct PbBatchBeam {
+    Frame f;
+    ProtonTables t;
+    const float *wet;  // smoothed WET of this beam (cm)
+    const float *mu;   // spot weights (nullptr: the table's MU)
+};
+
+struct PbBatchPlan {
+    Grid g;
+    float *dose;  // sum over the plan's beams
+    int beam0, n_beams;
+};
+
+// Work items are (plan, tile) pairs; tile = k * tiles_x * tiles_y + by * tiles_x + bx
+// for the variant's tile shape.  `next` is the device queue head (reset here).
+int pencil_beam_batch_variants();
+void pencil_beam_batch_tile(int variant, int *threads_y, int *voxels_y);
+void launch_pencil_beam_batch(DeviceContext &ctx, int variant, const PbBatchPlan *plans, const PbBatchBeam *beams,
+                              const int2 *items, int n_items, unsigned *next, int lut_len, cudaStream_t s);
+
 }  // namespace dc

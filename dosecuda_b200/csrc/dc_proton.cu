@@ -214,9 +214,10 @@ void launch_layer_rcut(const Grid &g, const Frame &f, LayerRec *layers, int n_la
 //   kPbSpotMax  spot_max[s]   = max_v K_s(v)
 //   kPbCount    counts[v]     = #{s : K_s(v) >= thr[s]}
 //   kPbFill     CSR row v     = (s, K_s(v)) for K_s(v) >= thr[s], in spot-table order
-template <int kMode>
-__global__ void __launch_bounds__(kPbThreadsX *kPbThreadsY)
-    pb_kernel(Grid g, Frame f, ProtonTables t, const float *__restrict__ wet_s, float *__restrict__ dose, PbExtra x) {
+template <int kMode, int TY, int VY>
+__device__ __forceinline__ void pb_tile(const Grid &g, const Frame &f, const ProtonTables &t,
+                                        const float *__restrict__ wet_s, int bx, int by, int k, float (&acc)[VY],
+                                        const PbExtra &x) {
     extern __shared__ float4 smem4[];
     float4 *s_spot_a = smem4;                    // x, y, mu, orig (int bits)
     float4 *s_spot_b = smem4 + kPbSpotChunk;     // tx, ty, inv_t2, threshold
@@ -226,24 +227,26 @@ __global__ void __launch_bounds__(kPbThreadsX *kPbThreadsY)
     float *s_sigma = s_lut + t.lut_len;
     float *s_idd = s_lut + 2 * t.lut_len;
 
+    constexpr int kThreads = kPbThreadsX * TY;
+    constexpr int kSpt = kPbSpotChunk / kThreads;  // spots tested per thread per staging round
+    static_assert(kSpt * kThreads == kPbSpotChunk, "staging round must cover the chunk");
     const int tid = threadIdx.y * kPbThreadsX + threadIdx.x;
     const int lane = threadIdx.x;
-    const int nthreads = kPbThreadsX * kPbThreadsY;
-    const int i = blockIdx.x * kPbThreadsX + threadIdx.x;
-    const int j0 = blockIdx.y * (kPbThreadsY * kPbVoxY) + threadIdx.y;
-    const int k = blockIdx.z;
+    const int nthreads = kThreads;
+    const int i = bx * kPbThreadsX + threadIdx.x;
+    const int j0 = by * (TY * VY) + threadIdx.y;
+    __syncthreads();  // shared memory of a previous tile (persistent caller) no longer in use
 
-    float hx[kPbVoxY], hy[kPbVoxY], hz[kPbVoxY], hz2[kPbVoxY], wet_mm[kPbVoxY], dsrc[kPbVoxY], acc[kPbVoxY];
-    float gv[kPbVoxY];
-    long long vidx[kPbVoxY];
-    long long fill_off[kPbVoxY], fill_end[kPbVoxY];
-    int cnt[kPbVoxY];
-    bool inside[kPbVoxY];
+    float hx[VY], hy[VY], hz[VY], hz2[VY], wet_mm[VY], dsrc[VY];
+    float gv[VY];
+    long long vidx[VY];
+    long long fill_off[VY], fill_end[VY];
+    int cnt[VY];
+    bool inside[VY];
 #pragma unroll
-    for (int v = 0; v < kPbVoxY; ++v) {
-        const int j = j0 + v * kPbThreadsY;
+    for (int v = 0; v < VY; ++v) {
+        const int j = j0 + v * TY;
         inside[v] = (i < g.nx) && (j < g.ny);
-        acc[v] = 0.0f;
         cnt[v] = 0;
         const int ic = min(i, g.nx - 1), jc = min(j, g.ny - 1);
         vidx[v] = (long long)ic + (long long)g.nx * (jc + (long long)g.ny * k);
@@ -265,13 +268,13 @@ __global__ void __launch_bounds__(kPbThreadsX *kPbThreadsY)
     }
 
     // Beam's-eye-view bounding box of the CTA's voxels (for spot culling).
-    __shared__ float s_red[kPbThreadsY][6];
+    __shared__ float s_red[TY][6];
     __shared__ float s_bb[6];
-    __shared__ int s_wcnt[kPbThreadsY];
+    __shared__ int s_wcnt[TY];
     {
         float b[6] = {INFINITY, -INFINITY, INFINITY, -INFINITY, INFINITY, -INFINITY};
 #pragma unroll
-        for (int v = 0; v < kPbVoxY; ++v) {
+        for (int v = 0; v < VY; ++v) {
             if (!inside[v]) continue;
             b[0] = fminf(b[0], hx[v]);
             b[1] = fmaxf(b[1], hx[v]);
@@ -295,7 +298,7 @@ __global__ void __launch_bounds__(kPbThreadsX *kPbThreadsY)
         __syncthreads();
         if (tid < 6) {
             float r = s_red[0][tid];
-            for (int w = 1; w < kPbThreadsY; ++w) r = (tid & 1) ? fmaxf(r, s_red[w][tid]) : fminf(r, s_red[w][tid]);
+            for (int w = 1; w < TY; ++w) r = (tid & 1) ? fmaxf(r, s_red[w][tid]) : fminf(r, s_red[w][tid]);
             s_bb[tid] = r;
         }
         __syncthreads();
@@ -315,11 +318,11 @@ __global__ void __launch_bounds__(kPbThreadsX *kPbThreadsY)
         }
         __syncthreads();
 
-        PbVoxel pv[kPbVoxY];
-        bool act[kPbVoxY];
+        PbVoxel pv[VY];
+        bool act[VY];
         bool any = false;
 #pragma unroll
-        for (int v = 0; v < kPbVoxY; ++v) {
+        for (int v = 0; v < VY; ++v) {
             act[v] = inside[v] && pb_voxel_layer(L, s_depth, s_sigma, s_idd, t.lut_len, wet_mm[v], dsrc[v], pv[v]);
             if (!act[v]) {
                 pv[v].pf = pv[v].hf = 0.f;
@@ -337,11 +340,11 @@ __global__ void __launch_bounds__(kPbThreadsX *kPbThreadsY)
             // Each thread tests two consecutive spots; the ones whose divergent
             // axis comes within rcut of the CTA's box are compacted in order.
             const float4 *gsp = reinterpret_cast<const float4 *>(t.spots + L.spot_start + c0);
-            float4 a2[2], b2[2];
-            bool keep[2];
+            float4 a2[kSpt], b2[kSpt];
+            bool keep[kSpt];
 #pragma unroll
-            for (int u = 0; u < 2; ++u) {
-                const int q = 2 * tid + u;
+            for (int u = 0; u < kSpt; ++u) {
+                const int q = kSpt * tid + u;
                 keep[u] = false;
                 if (q < craw) {
                     a2[u] = __ldg(gsp + 2 * q);
@@ -355,7 +358,9 @@ __global__ void __launch_bounds__(kPbThreadsX *kPbThreadsY)
                     keep[u] = !((dx * dx + dy * dy) * b2[u].z > rcut2);
                 }
             }
-            const int mine = (int)keep[0] + (int)keep[1];
+            int mine = 0;
+#pragma unroll
+            for (int u = 0; u < kSpt; ++u) mine += (int)keep[u];
             int incl = mine;
 #pragma unroll
             for (int o = 1; o < 32; o <<= 1) {
@@ -366,14 +371,14 @@ __global__ void __launch_bounds__(kPbThreadsX *kPbThreadsY)
             __syncthreads();
             int base = 0, cn = 0;
 #pragma unroll
-            for (int w = 0; w < kPbThreadsY; ++w) {
+            for (int w = 0; w < TY; ++w) {
                 const int c = s_wcnt[w];
                 base += (w < (int)threadIdx.y) ? c : 0;
                 cn += c;
             }
             int pos = base + incl - mine;
 #pragma unroll
-            for (int u = 0; u < 2; ++u) {
+            for (int u = 0; u < kSpt; ++u) {
                 if (!keep[u]) continue;
                 float4 a = a2[u], b = b2[u];
                 const int orig = __float_as_int(a.w);
@@ -388,15 +393,15 @@ __global__ void __launch_bounds__(kPbThreadsX *kPbThreadsY)
             if (cn == 0) continue;
             if (kMode == kPbDose) {
                 if (!any) continue;
-                float accp[kPbVoxY], acch[kPbVoxY];
+                float accp[VY], acch[VY];
 #pragma unroll
-                for (int v = 0; v < kPbVoxY; ++v) accp[v] = acch[v] = 0.f;
+                for (int v = 0; v < VY; ++v) accp[v] = acch[v] = 0.f;
 #pragma unroll 4
                 for (int q = 0; q < cn; ++q) {
                     const float4 a = s_spot_a[q];
                     const float4 b = s_spot_b[q];
 #pragma unroll
-                    for (int v = 0; v < kPbVoxY; ++v) {
+                    for (int v = 0; v < VY; ++v) {
                         const float rx = hx[v] - a.x;
                         const float ry = hy[v] - a.y;
                         const float ray2 = fmaf(rx, rx, fmaf(ry, ry, hz2[v]));
@@ -407,7 +412,7 @@ __global__ void __launch_bounds__(kPbThreadsX *kPbThreadsY)
                     }
                 }
 #pragma unroll
-                for (int v = 0; v < kPbVoxY; ++v) {
+                for (int v = 0; v < VY; ++v) {
                     if (act[v]) acc[v] += fmaf(pv[v].pf, accp[v], pv[v].hf * acch[v]);
                 }
             } else {
@@ -415,9 +420,9 @@ __global__ void __launch_bounds__(kPbThreadsX *kPbThreadsY)
                 for (int q = 0; q < cn; ++q) {
                     const float4 a = s_spot_a[q];
                     const float4 b = s_spot_b[q];
-                    float kv[kPbVoxY];
+                    float kv[VY];
 #pragma unroll
-                    for (int v = 0; v < kPbVoxY; ++v) {
+                    for (int v = 0; v < VY; ++v) {
                         const float rx = hx[v] - a.x;
                         const float ry = hy[v] - a.y;
                         const float ray2 = fmaf(rx, rx, fmaf(ry, ry, hz2[v]));
@@ -429,21 +434,23 @@ __global__ void __launch_bounds__(kPbThreadsX *kPbThreadsY)
                     if (kMode == kPbAdjoint) {
                         float c = 0.0f;
 #pragma unroll
-                        for (int v = 0; v < kPbVoxY; ++v) c = fmaf(gv[v], kv[v], c);
+                        for (int v = 0; v < VY; ++v) c = fmaf(gv[v], kv[v], c);
 #pragma unroll
                         for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
                         if (lane == 0 && c != 0.0f) atomicAdd(&s_acc[q], c);
                     } else if (kMode == kPbSpotMax) {
-                        float m = fmaxf(kv[0], kv[1]);
+                        float m = 0.0f;
+#pragma unroll
+                        for (int v = 0; v < VY; ++v) m = fmaxf(m, kv[v]);
 #pragma unroll
                         for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
                         if (lane == 0 && m > 0.0f) atomicMax(x.spot_max + __float_as_int(a.w), __float_as_uint(m));
                     } else if (kMode == kPbCount) {
 #pragma unroll
-                        for (int v = 0; v < kPbVoxY; ++v) cnt[v] += (act[v] && kv[v] >= b.w && kv[v] > 0.0f) ? 1 : 0;
+                        for (int v = 0; v < VY; ++v) cnt[v] += (act[v] && kv[v] >= b.w && kv[v] > 0.0f) ? 1 : 0;
                     } else if (kMode == kPbFill) {
 #pragma unroll
-                        for (int v = 0; v < kPbVoxY; ++v) {
+                        for (int v = 0; v < VY; ++v) {
                             if (act[v] && kv[v] >= b.w && kv[v] > 0.0f && fill_off[v] < fill_end[v]) {
                                 x.col[fill_off[v]] = __float_as_int(a.w);
                                 x.val[fill_off[v]] = kv[v];
@@ -463,32 +470,94 @@ __global__ void __launch_bounds__(kPbThreadsX *kPbThreadsY)
         }
     }
 
+    if (kMode == kPbCount) {
 #pragma unroll
-    for (int v = 0; v < kPbVoxY; ++v) {
-        if (!inside[v]) continue;
-        if (kMode == kPbDose) dose[vidx[v]] = acc[v];
-        if (kMode == kPbCount) x.counts[vidx[v]] = cnt[v];
+        for (int v = 0; v < VY; ++v)
+            if (inside[v]) x.counts[vidx[v]] = cnt[v];
     }
 }
 
-static size_t pb_smem(const ProtonTables &t) {
-    return 2 * kPbSpotChunk * sizeof(float4) + kPbSpotChunk * sizeof(float) + 3 * (size_t)t.lut_len * sizeof(float);
+
+// One tile per CTA (grid = tiles of the volume x slices).
+template <int kMode, int TY, int VY>
+__global__ void __launch_bounds__(kPbThreadsX *TY)
+    pb_kernel(Grid g, Frame f, ProtonTables t, const float *__restrict__ wet_s, float *__restrict__ dose, PbExtra x) {
+    float acc[VY];
+#pragma unroll
+    for (int v = 0; v < VY; ++v) acc[v] = 0.0f;
+    pb_tile<kMode, TY, VY>(g, f, t, wet_s, blockIdx.x, blockIdx.y, blockIdx.z, acc, x);
+    if (kMode == kPbDose) {
+        const int i = blockIdx.x * kPbThreadsX + threadIdx.x;
+#pragma unroll
+        for (int v = 0; v < VY; ++v) {
+            const int j = blockIdx.y * (TY * VY) + threadIdx.y + v * TY;
+            if (i < g.nx && j < g.ny) dose[(long long)i + (long long)g.nx * (j + (long long)g.ny * blockIdx.z)] = acc[v];
+        }
+    }
+}
+
+// Persistent batch kernel: CTAs take (plan, tile) work items from a device
+// queue (most expensive plans first) and sum the dose of all the plan's beams
+// for the tile in registers before one write per voxel.
+template <int TY, int VY>
+__global__ void __launch_bounds__(kPbThreadsX *TY)
+    pb_batch_kernel(const PbBatchPlan *__restrict__ plans, const PbBatchBeam *__restrict__ beams,
+                    const int2 *__restrict__ items, int n_items, unsigned *__restrict__ next) {
+    __shared__ int s_item;
+    while (true) {
+        __syncthreads();
+        if (threadIdx.x == 0 && threadIdx.y == 0) s_item = (int)atomicAdd(next, 1u);
+        __syncthreads();
+        const int it = s_item;
+        if (it >= n_items) break;
+        const int2 w = items[it];
+        const PbBatchPlan P = plans[w.x];
+        const int tiles_x = (P.g.nx + kPbThreadsX - 1) / kPbThreadsX;
+        const int tiles_y = (P.g.ny + TY * VY - 1) / (TY * VY);
+        const int k = w.y / (tiles_x * tiles_y);
+        const int rem = w.y - k * tiles_x * tiles_y;
+        const int by = rem / tiles_x, bx = rem - by * tiles_x;
+        float acc[VY];
+#pragma unroll
+        for (int v = 0; v < VY; ++v) acc[v] = 0.0f;
+        for (int b = P.beam0; b < P.beam0 + P.n_beams; ++b) {
+            const PbBatchBeam B = beams[b];
+            PbExtra x;
+            x.mu = B.mu;
+            pb_tile<kPbDose, TY, VY>(P.g, B.f, B.t, B.wet, bx, by, k, acc, x);
+        }
+        const int i = bx * kPbThreadsX + threadIdx.x;
+#pragma unroll
+        for (int v = 0; v < VY; ++v) {
+            const int j = by * (TY * VY) + threadIdx.y + v * TY;
+            if (i < P.g.nx && j < P.g.ny) P.dose[(long long)i + (long long)P.g.nx * (j + (long long)P.g.ny * k)] = acc[v];
+        }
+    }
+}
+
+static size_t pb_smem(int lut_len) {
+    return 2 * kPbSpotChunk * sizeof(float4) + kPbSpotChunk * sizeof(float) + 3 * (size_t)lut_len * sizeof(float);
+}
+
+template <class K>
+static void pb_attr(K kernel, size_t smem, int device, bool *done) {
+    if (smem > 48 * 1024 && device < 64 && !done[device]) {
+        DC_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+        done[device] = true;
+    }
 }
 
 template <int kMode>
 static void pb_launch(DeviceContext &ctx, const char *name, const Grid &g, const Frame &f, const ProtonTables &t,
                       const float *wet_s, float *dose, const PbExtra &x, cudaStream_t s) {
-    const size_t smem = pb_smem(t);
+    const size_t smem = pb_smem(t.lut_len);
     static bool attr_set[64] = {false};
-    if (smem > 48 * 1024 && ctx.device < 64 && !attr_set[ctx.device]) {
-        DC_CUDA(cudaFuncSetAttribute(pb_kernel<kMode>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
-        attr_set[ctx.device] = true;
-    }
+    pb_attr(pb_kernel<kMode, kPbThreadsY, kPbVoxY>, smem, ctx.device, attr_set);
     dim3 block(kPbThreadsX, kPbThreadsY, 1);
     dim3 grid((unsigned)((g.nx + kPbThreadsX - 1) / kPbThreadsX),
               (unsigned)((g.ny + kPbThreadsY * kPbVoxY - 1) / (kPbThreadsY * kPbVoxY)), (unsigned)g.nz);
     KernelTimer kt(ctx, name, s);
-    pb_kernel<kMode><<<grid, block, smem, s>>>(g, f, t, wet_s, dose, x);
+    pb_kernel<kMode, kPbThreadsY, kPbVoxY><<<grid, block, smem, s>>>(g, f, t, wet_s, dose, x);
     check_launch(name);
 }
 
@@ -507,6 +576,41 @@ void launch_pencil_beam_mode(DeviceContext &ctx, int mode, const Grid &g, const 
         case kPbCount: pb_launch<kPbCount>(ctx, "pencil_beam_count", g, f, t, wet_s, nullptr, x, s); break;
         case kPbFill: pb_launch<kPbFill>(ctx, "pencil_beam_fill", g, f, t, wet_s, nullptr, x, s); break;
         default: throw Error(DC_ERR_VALUE, "unknown pencil-beam mode");
+    }
+}
+
+// Tile shapes of the batch kernel (threads along y, voxels per thread along y).
+static const int kPbVariants[][2] = {{8, 2}, {4, 2}, {8, 1}, {4, 4}};
+int pencil_beam_batch_variants() { return (int)(sizeof(kPbVariants) / sizeof(kPbVariants[0])); }
+void pencil_beam_batch_tile(int variant, int *ty, int *vy) {
+    *ty = kPbVariants[variant][0];
+    *vy = kPbVariants[variant][1];
+}
+
+template <int TY, int VY>
+static void pb_batch_launch(DeviceContext &ctx, const PbBatchPlan *plans, const PbBatchBeam *beams,
+                            const int2 *items, int n_items, unsigned *next, int lut_len, cudaStream_t s) {
+    const size_t smem = pb_smem(lut_len);
+    static bool attr_set[64] = {false};
+    pb_attr(pb_batch_kernel<TY, VY>, smem, ctx.device, attr_set);
+    int sms = 0, per_sm = 0;
+    DC_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx.device));
+    DC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pb_batch_kernel<TY, VY>, kPbThreadsX * TY, smem));
+    const int blocks = std::max(1, std::min(n_items, sms * std::max(per_sm, 1)));
+    DC_CUDA(cudaMemsetAsync(next, 0, sizeof(unsigned), s));
+    KernelTimer kt(ctx, "pencil_beam_batch", s);
+    pb_batch_kernel<TY, VY><<<blocks, dim3(kPbThreadsX, TY, 1), smem, s>>>(plans, beams, items, n_items, next);
+    check_launch("pb_batch_kernel");
+}
+
+void launch_pencil_beam_batch(DeviceContext &ctx, int variant, const PbBatchPlan *plans, const PbBatchBeam *beams,
+                              const int2 *items, int n_items, unsigned *next, int lut_len, cudaStream_t s) {
+    switch (variant) {
+        case 0: pb_batch_launch<8, 2>(ctx, plans, beams, items, n_items, next, lut_len, s); break;
+        case 1: pb_batch_launch<4, 2>(ctx, plans, beams, items, n_items, next, lut_len, s); break;
+        case 2: pb_batch_launch<8, 1>(ctx, plans, beams, items, n_items, next, lut_len, s); break;
+        case 3: pb_batch_launch<4, 4>(ctx, plans, beams, items, n_items, next, lut_len, s); break;
+        default: throw Error(DC_ERR_VALUE, "unknown pencil-beam tile variant");
     }
 }
 

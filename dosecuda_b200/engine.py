@@ -247,3 +247,144 @@ def proton_dose_autograd(mu: torch.Tensor, wet: torch.Tensor, plan: ProtonBeamPl
     """Differentiable dose of one beam in its spot weights: forward is the
     pencil-beam kernel, backward the hand-written adjoint kernel (D^T g)."""
     return _ProtonDoseFn.apply(mu, wet, plan)
+
+
+class ProtonBatch:
+    """Many IMPT plans on one device, evaluated by one persistent launch.
+
+    ``add_plan(grid, rlsp)`` takes a CT grid (spacing/origin, any anisotropic
+    spacing) and its RLSP volume (CUDA tensor); ``add_beam(plan_id, beam)``
+    takes an IMPTBeam-like object (iso, gantry_angle, couch_angle,
+    spot_list).  After ``commit()``, ``wet()`` computes every beam's WET and
+    ``dose(mu)`` every plan's dose (``self.doses[plan_id]``); both only enqueue
+    device work, so they can be captured with ``torch.cuda.CUDAGraph``.
+    ``autotune()`` times the kernel's tile shapes on this workload and keeps
+    the fastest (cached in a JSON file keyed by the workload and GPU)."""
+
+    def __init__(self, model, device="cuda"):
+        dev = torch.device(device)
+        if dev.index is None:
+            dev = torch.device("cuda", torch.cuda.current_device())
+        self.device = dev
+        self.model = model
+        dvp = np.ascontiguousarray(model.divergence_params, dtype=np.float32)
+        luts = [np.ascontiguousarray(a, dtype=np.float32) for a in (model.lut_depths, model.lut_sigmas,
+                                                                    model.lut_idds)]
+        h = C.c_void_p()
+        with torch.cuda.device(dev):
+            rc = _lib.load().dc_proton_batch_create(
+                dev.index, dvp.ctypes.data_as(C.c_void_p), dvp.shape[0], dvp.shape[1],
+                luts[0].ctypes.data_as(C.c_void_p), luts[1].ctypes.data_as(C.c_void_p),
+                luts[2].ctypes.data_as(C.c_void_p), luts[0].shape[1], float(model.VSADX), float(model.VSADY),
+                C.byref(h))
+        _lib.raise_for(rc)
+        self._h = h
+        self.rlsp, self.doses, self.wets, self.beam_plan, self.beam_spots = [], [], [], [], []
+        self.variant = 0
+        self.committed = False
+
+    def add_plan(self, grid, rlsp: torch.Tensor) -> int:
+        _check_volume(rlsp, "rlsp")
+        dose = torch.zeros_like(rlsp)
+        pid = C.c_int()
+        nz, ny, nx = rlsp.shape
+        sp = np.asarray(grid.spacing, dtype=np.float32).reshape(-1)
+        sp3 = (sp[0], sp[0], sp[0]) if sp.size == 1 else (sp[0], sp[1], sp[2])
+        _lib.raise_for(_lib.load().dc_proton_batch_add_plan(self._h, nz, ny, nx, _lib.f3(sp3), _lib.f3(grid.origin),
+                                                            C.c_void_p(rlsp.data_ptr()), C.c_void_p(dose.data_ptr()),
+                                                            C.byref(pid)))
+        self.rlsp.append(rlsp)
+        self.doses.append(dose)
+        return pid.value
+
+    def add_beam(self, plan_id: int, beam) -> int:
+        wet = torch.empty_like(self.rlsp[plan_id])
+        sp = np.ascontiguousarray(beam.spot_list, dtype=np.float32).reshape(-1, 4)
+        bid = C.c_int()
+        _lib.raise_for(_lib.load().dc_proton_batch_add_beam(
+            self._h, plan_id, _lib.f3(beam.iso), float(beam.gantry_angle), float(beam.couch_angle),
+            sp.ctypes.data_as(C.c_void_p), sp.shape[0], C.c_void_p(wet.data_ptr()), C.byref(bid)))
+        self.wets.append(wet)
+        self.beam_plan.append(plan_id)
+        self.beam_spots.append(sp)
+        return bid.value
+
+    def commit(self):
+        lib = _lib.load()
+        _lib.raise_for(lib.dc_proton_batch_commit(self._h))
+        n = [C.c_int() for _ in range(4)]
+        _lib.raise_for(lib.dc_proton_batch_info(self._h, *[C.byref(x) for x in n]))
+        self.n_plans, self.n_beams, self.n_spots, self.n_variants = (x.value for x in n)
+        offs = []
+        for b in range(self.n_beams):
+            o = C.c_int()
+            _lib.raise_for(lib.dc_proton_batch_beam_spot_offset(self._h, b, C.byref(o)))
+            offs.append(o.value)
+        self.spot_offsets = offs
+        mu = np.zeros(self.n_spots, np.float32)
+        for b, sp in enumerate(self.beam_spots):
+            mu[offs[b]:offs[b] + sp.shape[0]] = sp[:, 2]
+        self.mu0 = torch.as_tensor(mu, device=self.device)
+        self.committed = True
+        return self
+
+    def wet(self, stream=None):
+        s = stream if stream is not None else torch.cuda.current_stream(self.device)
+        _lib.raise_for(_lib.load().dc_proton_batch_wet(self._h, C.c_void_p(s.cuda_stream)))
+
+    def dose(self, mu: torch.Tensor | None = None, variant: int | None = None, stream=None):
+        s = stream if stream is not None else torch.cuda.current_stream(self.device)
+        mp = None
+        if mu is not None:
+            if mu.device != self.device or mu.dtype != torch.float32 or not mu.is_contiguous() or \
+                    mu.numel() != self.n_spots:
+                raise ValueError("mu must be a contiguous float32 tensor with one weight per spot on the batch's device")
+            mp = C.c_void_p(mu.data_ptr())
+        v = self.variant if variant is None else variant
+        _lib.raise_for(_lib.load().dc_proton_batch_dose(self._h, mp, int(v), C.c_void_p(s.cuda_stream)))
+        return self.doses
+
+    def autotune(self, cache_path: str | None = None, repeats: int = 3) -> int:
+        """Time every tile shape of the batch dose kernel on this workload and
+        keep the fastest; results are cached in ``cache_path`` (JSON)."""
+        import json
+        import os
+        key = "%s|%d plans|%d beams|%d spots|%s" % (
+            torch.cuda.get_device_name(self.device), self.n_plans, self.n_beams, self.n_spots,
+            ";".join("x".join(str(d) for d in r.shape) for r in self.rlsp))
+        cache = {}
+        if cache_path and os.path.exists(cache_path):
+            with open(cache_path) as f:
+                cache = json.load(f)
+        if key in cache:
+            self.variant = int(cache[key]["variant"])
+            return self.variant
+        times = []
+        for v in range(self.n_variants):
+            self.dose(variant=v)
+            torch.cuda.synchronize(self.device)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            for _ in range(repeats):
+                self.dose(variant=v)
+            b.record()
+            torch.cuda.synchronize(self.device)
+            times.append(a.elapsed_time(b) / repeats)
+        self.variant = int(np.argmin(times))
+        if cache_path:
+            cache[key] = {"variant": self.variant, "ms": times}
+            with open(cache_path, "w") as f:
+                json.dump(cache, f, indent=1)
+        self.tune_ms = times
+        return self.variant
+
+    def close(self):
+        if self._h:
+            _lib.load().dc_proton_batch_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

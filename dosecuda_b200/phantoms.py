@@ -113,3 +113,106 @@ def volume_object(grid, data):
     v.origin = np.array(grid.origin, dtype=np.single)
     v.spacing = np.array(grid.spacing, dtype=np.single)
     return v
+
+
+# ---------------------------------------------------------------------------
+# Batched IMPT workload: patient-like phantoms with a spherical target
+# ---------------------------------------------------------------------------
+def _axis_wet_profile(rlsp, spacing, origin, src, iso, step_mm=1.0):
+    """WET (mm) along the line from the source through the isocentre, as a
+    function of distance from the source (nearest-voxel samples)."""
+    nz, ny, nx = rlsp.shape
+    sp = np.asarray(spacing, np.float64)
+    d = np.asarray(iso, np.float64) - np.asarray(src, np.float64)
+    L = np.linalg.norm(d)
+    u = d / L
+    t = np.arange(0.0, L + 400.0, step_mm)
+    pts = np.asarray(src, np.float64)[None, :] + t[:, None] * u[None, :]
+    ijk = np.rint((pts - np.asarray(origin, np.float64)[None, :]) / sp[None, :]).astype(np.int64)
+    inside = (ijk[:, 0] >= 0) & (ijk[:, 0] < nx) & (ijk[:, 1] >= 0) & (ijk[:, 1] < ny) & (ijk[:, 2] >= 0) & \
+             (ijk[:, 2] < nz)
+    rho = np.zeros(len(t))
+    rho[inside] = rlsp[ijk[inside, 2], ijk[inside, 1], ijk[inside, 0]]
+    return t, np.cumsum(np.maximum(rho, 0.0)) * step_mm
+
+
+def batch_plan(seed=0, shape=(160, 256, 256), spacing=(1.5, 1.5, 2.0), model=None, pitch_range=(4.0, 6.0),
+               max_beams=3, max_spots=12000):
+    """(IMPTDoseGrid, [IMPTBeam], target (centre, radius)) of one plan of the
+    batched workload: a water-equivalent body ellipsoid (20 +- 40 HU) with 1-6
+    random bone/lung/air ellipsoids (1000, -750, -1000 HU; semi-axes 5-40 mm)
+    and a spherical target (r 20-45 mm); 1-3 beams at uniform gantry angles;
+    energy layers covering the target at 3 mm R80 spacing; spots on a 4-6 mm
+    grid over the target's projection; weights lognormal(0, 0.5)."""
+    rng = np.random.default_rng(seed)
+    nz, ny, nx = shape
+    sx, sy, sz = spacing
+    grid = IMPTDoseGrid()
+    grid.origin = np.array([-nx * sx / 2.0, -ny * sy / 2.0, -nz * sz / 2.0])
+    grid.spacing = np.array([sx, sy, sz])
+    grid.size = np.array(shape)
+    z = (np.arange(nz) + 0.5) * sz + grid.origin[2]
+    y = (np.arange(ny) + 0.5) * sy + grid.origin[1]
+    x = (np.arange(nx) + 0.5) * sx + grid.origin[0]
+    Z, Y, X = np.meshgrid(z.astype(np.float32), y.astype(np.float32), x.astype(np.float32), indexing="ij")
+    ext = np.array([nx * sx, ny * sy, nz * sz]) / 2.0
+    body_ax = ext * rng.uniform(0.78, 0.92, size=3)
+    body = (X / body_ax[0]) ** 2 + (Y / body_ax[1]) ** 2 + (Z / body_ax[2]) ** 2 <= 1.0
+    hu = np.full(shape, -1000.0, np.float32)
+    hu[body] = (20.0 + 40.0 * rng.standard_normal(int(body.sum()))).astype(np.float32)
+    for _ in range(int(rng.integers(1, 7))):
+        c = rng.uniform(-0.5, 0.5, size=3) * body_ax
+        a = rng.uniform(5.0, 40.0, size=3)
+        val = float(rng.choice([1000.0, -750.0, -1000.0]))
+        m = ((X - c[0]) / a[0]) ** 2 + ((Y - c[1]) / a[1]) ** 2 + ((Z - c[2]) / a[2]) ** 2 <= 1.0
+        hu[m & body] = val
+    r_t = float(rng.uniform(20.0, 45.0))
+    c_t = rng.uniform(-0.25, 0.25, size=3) * np.maximum(body_ax - r_t - 10.0, 0.0)
+    tgt = ((X - c_t[0]) ** 2 + (Y - c_t[1]) ** 2 + (Z - c_t[2]) ** 2) <= r_t ** 2
+    hu[tgt] = (20.0 + 40.0 * rng.standard_normal(int(tgt.sum()))).astype(np.float32)
+    grid.HU = hu
+
+    if model is None:
+        model = IMPTPlan().beam_models[0]
+    rlsp = grid.RLSPFromHU("HitachiProbeatJHU")
+    r80 = np.asarray(model.divergence_params[:, 1], np.float64)
+    sad = (float(model.VSADX) + float(model.VSADY)) / 2.0
+    beams = []
+    total = 0
+    for _ in range(int(rng.integers(1, max_beams + 1))):
+        ga = float(rng.uniform(0.0, 360.0))
+        # source position for gantry ga (+180 inside the engine), couch 0
+        g = np.deg2rad(np.float32((ga + 180.0) % 360.0))
+        src = c_t + np.array([-sad * np.sin(g), sad * np.cos(g), 0.0])
+        t, wet = _axis_wet_profile(rlsp, grid.spacing, grid.origin, src, c_t)
+        dist = np.linalg.norm(c_t - src)
+        w_prox = float(np.interp(dist - r_t, t, wet))
+        w_dist = float(np.interp(dist + r_t, t, wet))
+        ids = []
+        for w in np.arange(w_prox, w_dist + 3.0, 3.0):
+            e = int(np.argmin(np.abs(r80 - w)))
+            if e not in ids:
+                ids.append(e)
+        pitch = float(rng.uniform(*pitch_range))
+        n = int(np.ceil((r_t + 5.0) / pitch))
+        pos = np.arange(-n, n + 1) * pitch
+        gx, gy = np.meshgrid(pos, pos, indexing="xy")
+        keep = gx ** 2 + gy ** 2 <= (r_t + 5.0) ** 2
+        gx, gy = gx[keep], gy[keep]
+        rows = []
+        for e in ids:
+            mu = rng.lognormal(0.0, 0.5, size=gx.size)
+            rows.append(np.column_stack((gx, gy, mu, np.full(gx.size, e))))
+        spots = np.array(np.vstack(rows), dtype=np.single)
+        if beams and total + spots.shape[0] > max_spots:
+            break  # keep the plan within its spot budget
+        total += spots.shape[0]
+        beam = IMPTBeam()
+        beam.spot_list = spots
+        beam.n_spots = beam.spot_list.shape[0]
+        beam.gantry_angle = ga
+        beam.couch_angle = 0.0
+        beam.iso = np.array(c_t, dtype=np.single)
+        beam.dicom_rangeshifter_label = "0"
+        beams.append(beam)
+    return grid, beams, (c_t, r_t)

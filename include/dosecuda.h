@@ -238,6 +238,39 @@ int dc_proton_beam_influence_csr(dc_proton_beam *beam, const float *wet_dev, flo
                                  long long capacity, void *stream);
 
 /* ------------------------------------------------------------------ */
+/* Many IMPT plans in one persistent launch.  No counterpart in the     */
+/* reference, which computes one beam per call (plan_impt.py:139-160).  */
+/* Plans (CT grid, RLSP and dose volumes on the device) and beams       */
+/* (geometry, host spot list, device WET volume) are added, then        */
+/* committed (tables, work queues and textures are built); after that   */
+/* the WET and dose calls only enqueue device work on `stream`, so they */
+/* can be captured into a CUDA graph.  All beams share one beam model.  */
+/* ------------------------------------------------------------------ */
+typedef struct dc_proton_batch dc_proton_batch;
+
+int dc_proton_batch_create(int gpu_id, const float *divergence_params, int n_energies, int dvp_len,
+                           const float *lut_depths, const float *lut_sigmas, const float *lut_idds,
+                           int lut_len, float vsadx, float vsady, dc_proton_batch **out);
+int dc_proton_batch_add_plan(dc_proton_batch *batch, int nz, int ny, int nx, const float spacing[3],
+                             const float origin[3], const float *rlsp_dev, float *dose_dev, int *plan_id);
+int dc_proton_batch_add_beam(dc_proton_batch *batch, int plan_id, const float iso[3], double gantry_deg,
+                             float couch_deg, const float *spots, int n_spots, float *wet_dev, int *beam_id);
+int dc_proton_batch_commit(dc_proton_batch *batch);
+/* n_variants: tile shapes the dose call accepts (for autotuning). */
+int dc_proton_batch_info(const dc_proton_batch *batch, int *n_plans, int *n_beams, int *n_spots_total,
+                         int *n_variants);
+/* Offset of a beam's spots in the batch's spot-weight vector. */
+int dc_proton_batch_beam_spot_offset(const dc_proton_batch *batch, int beam_id, int *offset);
+/* WET (ray march + smoothing) of every beam into its WET volume. */
+int dc_proton_batch_wet(dc_proton_batch *batch, void *stream);
+/* Dose of every plan (sum of its beams) into its dose volume.  mu_dev:
+ * n_spots_total weights on the device (beam by beam, each in its spot
+ * list's order), or NULL to reuse the previous weights (initially the MU
+ * column of the spot lists). */
+int dc_proton_batch_dose(dc_proton_batch *batch, const float *mu_dev, int variant, void *stream);
+int dc_proton_batch_destroy(dc_proton_batch *batch);
+
+/* ------------------------------------------------------------------ */
 /* Photon: ray trace + TERMA + collapsed-cone convolution/superposition */
 /* Replaces dose_kernels.photon_dose_cuda                               */
 /* (dosemodule.cu:377-557 -> IMRTClasses.cu:353-405).                   */

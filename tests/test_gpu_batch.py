@@ -1,0 +1,102 @@
+"""Batched IMPT: many plans (anisotropic grids, uneven beam and spot counts)
+in one persistent launch.  Oracles: per-plan, per-beam calls of the existing
+entry points, and the CPU oracle on one anisotropic plan; plus tile-shape
+variants, the autotuner and CUDA-graph replay."""
+import numpy as np
+import pytest
+
+from dosecheck import dose_diff
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def batch():
+    torch = pytest.importorskip("torch")
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from dosecuda_b200 import engine, phantoms
+    from dosecuda_b200.plan_impt import IMPTPlan
+    model = IMPTPlan().beam_models[0]
+    b = engine.ProtonBatch(model)
+    plans = []
+    for seed, shape, sp in ((1, (36, 44, 40), (3.0, 3.0, 4.0)), (2, (40, 40, 48), (3.0, 3.0, 3.0)),
+                            (3, (32, 48, 44), (3.5, 3.0, 4.0))):
+        grid, beams, _ = phantoms.batch_plan(seed, shape=shape, spacing=sp, model=model, pitch_range=(7.0, 9.0),
+                                             max_spots=4000)
+        rl = torch.from_numpy(grid.RLSPFromHU("HitachiProbeatJHU")).cuda()
+        pid = b.add_plan(grid, rl)
+        ids = [b.add_beam(pid, bm) for bm in beams]
+        plans.append((grid, beams, rl, pid, ids))
+    b.commit()
+    b.wet()
+    b.dose()
+    torch.cuda.synchronize()
+    return torch, engine, model, b, plans
+
+
+def test_batch_matches_per_beam_calls(batch):
+    torch, engine, model, b, plans = batch
+    dm = engine.ProtonModelDevice(model)
+    for grid, beams, rl, pid, ids in plans:
+        ref = torch.zeros_like(rl)
+        for bm, bid in zip(beams, ids):
+            w = engine.proton_wet(rl, grid, bm, model)
+            torch.cuda.synchronize()
+            assert torch.equal(w, b.wets[bid])  # the batch's WET is the per-beam WET
+            ref += engine.proton_dose(w, grid, bm, dm)
+        torch.cuda.synchronize()
+        assert dose_diff(b.doses[pid].cpu().numpy(), ref.cpu().numpy()) <= 1e-5
+
+
+def test_batch_anisotropic_plan_matches_oracle(batch):
+    import oracle
+    torch, engine, model, b, plans = batch
+    grid, beams, rl, pid, ids = plans[0]
+    sp = np.asarray(grid.spacing, np.float32)
+    ref = np.zeros(rl.shape)
+    for bm, bid in zip(beams, ids):
+        w = b.wets[bid].cpu().numpy()
+        o, _ = oracle.proton_dose(w, sp, grid.origin, bm.iso, bm.gantry_angle, bm.couch_angle, model, bm.spot_list)
+        ref += o
+    assert dose_diff(b.doses[pid].cpu().numpy(), ref) <= 1e-3
+
+
+def test_tile_variants_agree_and_autotune(batch, tmp_path):
+    torch, engine, model, b, plans = batch
+    base = [d.clone() for d in b.dose(variant=0)]
+    for v in range(1, b.n_variants):
+        out = b.dose(variant=v)
+        torch.cuda.synchronize()
+        for d0, d in zip(base, out):
+            assert dose_diff(d.cpu().numpy(), d0.cpu().numpy()) <= 1e-5
+    cache = tmp_path / "tune.json"
+    v = b.autotune(str(cache))
+    assert 0 <= v < b.n_variants and cache.exists()
+    assert b.autotune(str(cache)) == v  # served from the cache
+
+
+def test_weights_and_cuda_graph_replay(batch):
+    torch, engine, model, b, plans = batch
+    mu = b.mu0.clone()
+    b.dose(mu)
+    torch.cuda.synchronize()
+    d1 = [d.clone() for d in b.doses]
+    mu2 = (2.0 * b.mu0).contiguous()
+    g = torch.cuda.CUDAGraph()
+    s = torch.cuda.Stream()
+    s.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(s):
+        b.dose(mu2)  # warm-up on the capture stream
+    torch.cuda.current_stream().wait_stream(s)
+    torch.cuda.synchronize()
+    with torch.cuda.graph(g):
+        b.dose(mu2)
+    for _ in range(2):
+        for d in b.doses:
+            d.zero_()
+        g.replay()
+        torch.cuda.synchronize()
+        for d, r in zip(b.doses, d1):
+            assert dose_diff(d.cpu().numpy(), 2.0 * r.cpu().numpy()) <= 1e-5
+    del g
