@@ -360,6 +360,174 @@ def run_mine(args, ws, rank, local, dist_mod):
     return out
 
 
+def run_batched(args, local, dist_mod, ws):
+    """Batched IMPT: 16 patient-like plans (256x256x160 at 1.5x1.5x2.0 mm,
+    1-3 beams, 500-12,000 spots each) in one persistent launch, against the
+    same beams evaluated by per-beam calls of the drop-in API."""
+    import torch
+    from dosecuda_b200 import dose_kernels, engine, phantoms
+    from dosecuda_b200.plan import VolumeObject
+    from dosecuda_b200.plan_impt import IMPTPlan
+    dev = torch.device("cuda", local)
+    model = IMPTPlan().beam_models[0]
+    t0 = time.perf_counter()
+    plans = [phantoms.batch_plan(seed + 1000 * local, model=model) for seed in range(args.batch_plans)]
+    gen_s = time.perf_counter() - t0
+    b = engine.ProtonBatch(model, device=dev)
+    rls = []
+    for grid, beams, _ in plans:
+        rl = torch.from_numpy(grid.RLSPFromHU("HitachiProbeatJHU")).to(dev)
+        rls.append(rl)
+        pid = b.add_plan(grid, rl)
+        for bm in beams:
+            b.add_beam(pid, bm)
+    b.commit()
+    b.wet()
+    torch.cuda.synchronize()
+    variant = b.autotune(os.path.join(ROOT, "_build_autotune.json") if args.tune_cache else None)
+    for _ in range(args.warmup):
+        b.dose()
+    torch.cuda.synchronize()
+    barrier(dist_mod)
+    a, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(args.steps):
+        b.dose()
+    e.record()
+    torch.cuda.synchronize()
+    t_batch = aggregate_max(a.elapsed_time(e) / args.steps, dist_mod)
+    # the same launch replayed from a CUDA graph
+    g = torch.cuda.CUDAGraph()
+    side = torch.cuda.Stream(device=dev)
+    side.wait_stream(torch.cuda.current_stream(dev))
+    with torch.cuda.stream(side):
+        b.dose()
+    torch.cuda.current_stream(dev).wait_stream(side)
+    torch.cuda.synchronize()
+    with torch.cuda.graph(g):
+        b.dose()
+    g.replay()
+    torch.cuda.synchronize()
+    a.record()
+    for _ in range(args.steps):
+        g.replay()
+    e.record()
+    torch.cuda.synchronize()
+    t_graph = aggregate_max(a.elapsed_time(e) / args.steps, dist_mod)
+    del g
+    # per-plan calls: every beam through dose_kernels.proton_spot_cuda (host buffers)
+    wets = [w.cpu().numpy() for w in b.wets]
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    bi = 0
+    for (grid, beams, _), rl in zip(plans, rls):
+        vol = VolumeObject()
+        vol.voxel_data = grid.HU  # the reference's call also reads the RLSP volume; its content is unused
+        vol.origin = np.asarray(grid.origin, np.float32)
+        vol.spacing = np.asarray(grid.spacing, np.float32)
+        for bm in beams:
+            wv = VolumeObject()
+            wv.voxel_data, wv.origin, wv.spacing = wets[bi], vol.origin, vol.spacing
+            # per-axis spacing is not expressible through the reference's call (it uses spacing[0]);
+            # the timing of the call is what is compared here
+            dose_kernels.proton_spot_cuda(model, vol, wv, bm, local)
+            bi += 1
+    t_calls = aggregate_max((time.perf_counter() - t0) * 1e3, dist_mod)
+    n_spots = b.n_spots
+    out = {
+        "metric": "batched IMPT dose: ms per optimisation iteration (all plans)",
+        "value": round(t_batch, 3), "unit": "ms/iteration", "higher_is_better": False,
+        "graph_replay_ms": round(t_graph, 3),
+        "spots_per_s": round(n_spots * ws / (t_batch * 1e-3), 1),
+        "per_plan_calls_ms": round(t_calls, 3),
+        "speedup_vs_per_plan_calls": round(t_calls / t_batch, 2),
+        "tile_variant": int(variant), "tile_ms": [round(x, 3) for x in getattr(b, "tune_ms", [])],
+        "config": {"workload": "%d plans x 256x256x160 @ 1.5x1.5x2.0 mm, %d beams, %d spots; body ellipsoid "
+                               "(20+-40 HU) with bone/lung/air ellipsoids, spherical target, layers at 3 mm R80 "
+                               "spacing, 4-6 mm spot grid, lognormal(0, 0.5) weights" %
+                               (args.batch_plans, b.n_beams, n_spots),
+                   "iteration": "dose of every plan for new spot weights (WET resident)",
+                   "per_plan_calls": "one dose_kernels.proton_spot_cuda call per beam, host buffers"},
+        "generation_s": round(gen_s, 2),
+    }
+    b.close()
+    return out
+
+
+def run_optimisation(args, local, dist_mod):
+    """Differentiable IMPT optimisation: 3 beams, ~7,500 spots; objective
+    sum_target (D - 2 Gy)^2 + 10 sum_OAR max(D - 1 Gy, 0)^2 in FP64; gradient
+    by the adjoint kernel through torch.autograd; 200 projected-Adam
+    iterations."""
+    import torch
+    from dosecuda_b200 import engine, phantoms
+    from dosecuda_b200.plan_impt import IMPTPlan
+    dev = torch.device("cuda", local)
+    model = IMPTPlan().beam_models[0]
+    grid, beams, (c_t, r_t) = phantoms.batch_plan(102, model=model, n_beams=3)
+    rl = torch.from_numpy(grid.RLSPFromHU("HitachiProbeatJHU")).to(dev)
+    nz, ny, nx = rl.shape
+    sp = np.asarray(grid.spacing, np.float64)
+    zz = torch.arange(nz, device=dev, dtype=torch.float64) * sp[2] + grid.origin[2]
+    yy = torch.arange(ny, device=dev, dtype=torch.float64) * sp[1] + grid.origin[1]
+    xx = torch.arange(nx, device=dev, dtype=torch.float64) * sp[0] + grid.origin[0]
+    Z, Y, X = torch.meshgrid(zz, yy, xx, indexing="ij")
+    target = ((X - c_t[0]) ** 2 + (Y - c_t[1]) ** 2 + (Z - c_t[2]) ** 2) <= r_t ** 2
+    # OAR: cylinder r = 10 mm along z, adjacent to the target
+    oar = ((X - (c_t[0] + r_t + 10.0)) ** 2 + (Y - c_t[1]) ** 2) <= 10.0 ** 2
+    oar &= (Z - c_t[2]).abs() <= r_t
+    del X, Y, Z
+    plans = [engine.ProtonBeamPlan(grid, bm, model, device=dev) for bm in beams]
+    wets = [engine.proton_wet(rl, grid, bm, model) for bm in beams]
+    mus = [p.mu.clone() for p in plans]
+    with torch.no_grad():
+        d0 = sum(p.dose(w, m) for p, w, m in zip(plans, wets, mus))
+        scale = 2.0 / d0.double()[target].mean().item()
+    mu = torch.cat(mus) * scale
+    sizes = [p.n_spots for p in plans]
+
+    def dose_of(m):
+        parts = torch.split(m, sizes)
+        return sum(engine.proton_dose_autograd(q.contiguous(), w, p) for q, w, p in zip(parts, wets, plans))
+
+    def objective(d):
+        d = d.double()
+        return ((d[target] - 2.0) ** 2).sum() + 10.0 * (torch.clamp(d[oar] - 1.0, min=0.0) ** 2).sum()
+
+    mu = mu.detach().requires_grad_(True)
+    opt = torch.optim.Adam([mu], lr=0.02 * mu.detach().mean().item())
+    f0 = objective(dose_of(mu)).item()
+    iters = args.opt_iters
+    for _ in range(3):  # warm-up
+        f = objective(dose_of(mu))
+        f.backward()
+        mu.grad = None
+    torch.cuda.synchronize()
+    barrier(dist_mod)
+    a, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(iters):
+        opt.zero_grad(set_to_none=True)
+        f = objective(dose_of(mu))
+        f.backward()
+        opt.step()
+        with torch.no_grad():
+            mu.clamp_(min=0.0)
+    e.record()
+    torch.cuda.synchronize()
+    t = aggregate_max(a.elapsed_time(e) / iters, dist_mod)
+    f1 = objective(dose_of(mu)).item()
+    return {
+        "metric": "IMPT plan optimisation: ms per iteration (dose + adjoint + Adam step)",
+        "value": round(t, 3), "unit": "ms/iteration", "higher_is_better": False,
+        "iterations": iters, "objective_start": round(f0, 3), "objective_end": round(f1, 3),
+        "config": {"workload": "256x256x160 @ 1.5x1.5x2.0 mm, 3 beams, %d spots; target sphere r=%.1f mm, OAR "
+                               "cylinder r=10 mm adjacent" % (sum(sizes), r_t),
+                   "objective": "sum_target (D-2)^2 + 10 sum_OAR max(D-1,0)^2, FP64 reduction",
+                   "gradient": "hand-written adjoint kernel (D^T g) behind torch.autograd"},
+    }
+
+
 def cpu_baseline_photon():
     """The FP64 C oracle on the host cores: one full control point of the
     photon workload (the whole 128^3 beam; about 10-30 s of CPU time).
@@ -395,6 +563,8 @@ def main_mine(args):
     ws, rank, local = dist_env()
     dist_mod = init_dist(ws, "nccl" if torch.cuda.is_available() else "gloo")
     r = run_mine(args, ws, rank, local, dist_mod)
+    batched = run_batched(args, local, dist_mod, ws) if args.batch_plans > 0 else None
+    optimisation = run_optimisation(args, local, dist_mod) if args.opt_iters > 0 else None
     if rank == 0:
         cpu_x = cpu_p = None
         if ws == 1 and not args.no_cpu:
@@ -473,6 +643,8 @@ def main_mine(args):
                 "gpu_launches": p_launch_per_step * args.steps,
                 "cpu_baseline": cpu_p,
             },
+            "batched": batched,
+            "optimisation": optimisation,
         }
         print(json.dumps(line))
     if dist_mod is not None:
@@ -526,6 +698,37 @@ def main_reference(args):
         beam_step()
     p_s = (time.perf_counter() - t0) / args.steps
     n_spots = pbeam.spot_list.shape[0]
+
+    batched = None
+    if args.batch_plans > 0:
+        # the batched workload as the reference computes it: one call per beam,
+        # its WET kept between calls (computeIMPTPlanFromWET, plan_impt.py:192-211)
+        from dosecuda_b200 import phantoms
+        from dosecuda_b200.plan_impt import IMPTPlan
+        bmodel = IMPTPlan().beam_models[0]
+        calls = []
+        for seed in range(args.batch_plans):
+            grid, beams, _ = phantoms.batch_plan(seed, model=bmodel)
+            rv = VolumeObject()
+            rv.voxel_data = grid.RLSPFromHU("HitachiProbeatJHU")
+            rv.origin = np.asarray(grid.origin, np.float32)
+            rv.spacing = np.asarray(grid.spacing, np.float32)
+            for bm in beams:
+                wv = VolumeObject()
+                wv.voxel_data = ref.proton_raytrace_cuda(bmodel, rv, bm, local)
+                wv.origin, wv.spacing = rv.origin, rv.spacing
+                calls.append((rv, wv, bm))
+        ref.proton_spot_cuda(bmodel, *calls[0][:2], calls[0][2], local)  # warm-up
+        t0 = time.perf_counter()
+        for rv, wv, bm in calls:
+            ref.proton_spot_cuda(bmodel, rv, wv, bm, local)
+        t_calls = (time.perf_counter() - t0) * 1e3
+        batched = {"metric": "batched IMPT dose: ms per optimisation iteration (all plans)",
+                   "value": round(t_calls, 3), "unit": "ms/iteration", "higher_is_better": False,
+                   "config": {"workload": "%d plans x 256x256x160 (same seeds as the engine's line), %d beams; "
+                                          "the reference uses spacing[0] on all axes" % (args.batch_plans, len(calls)),
+                              "iteration": "one proton_spot_cuda call per beam, WET reused"}}
+
     line = {
         "impl": "reference",
         "metric": "CCCS ms/beam",
@@ -553,6 +756,7 @@ def main_reference(args):
         "secondary": {"metric": "IMPT spots/s", "value": round(n_spots / p_s, 1), "unit": "spots/s",
                       "higher_is_better": True, "ms_per_step": round(p_s * 1e3, 4),
                       "e2e": {"value": round(n_spots / p_s, 1), "unit": "spots/s"}},
+        "batched": batched,
     }
     print(json.dumps(line))
 
@@ -564,6 +768,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="mine", choices=["mine", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU oracle baseline")
+    ap.add_argument("--batch-plans", type=int, default=16, help="plans in the batched workload (0: skip)")
+    ap.add_argument("--opt-iters", type=int, default=200, help="optimisation iterations (0: skip)")
+    ap.add_argument("--tune-cache", action="store_true", help="keep the tile autotuner's JSON cache")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

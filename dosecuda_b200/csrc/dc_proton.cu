@@ -307,6 +307,26 @@ __device__ __forceinline__ void pb_tile(const Grid &g, const Frame &f, const Pro
 
     for (int l = 0; l < t.n_layers; ++l) {
         const LayerRec L = t.layers[l];
+        // Cheap whole-CTA skips before any staging: no voxel within the
+        // layer's range, or no spot of the layer within rcut of the CTA.
+        {
+            bool in_range = false;
+#pragma unroll
+            for (int v = 0; v < VY; ++v) in_range |= inside[v] && !(wet_mm[v] > 1.1f * L.r80);
+            if (!__syncthreads_or(in_range)) continue;
+            const float rc2 = L.rcut * L.rcut;
+            int near = 0;
+            for (int q = tid; q < L.n_spots; q += nthreads) {
+                const float4 *sp = reinterpret_cast<const float4 *>(t.spots + L.spot_start + q);
+                const float4 a = __ldg(sp), b = __ldg(sp + 1);
+                const float ax0 = a.x - b.x * bz0, ax1 = a.x - b.x * bz1;
+                const float ay0 = a.y - b.y * bz0, ay1 = a.y - b.y * bz1;
+                const float dx = fmaxf(0.0f, fmaxf(fminf(ax0, ax1) - bx1, bx0 - fmaxf(ax0, ax1)));
+                const float dy = fmaxf(0.0f, fmaxf(fminf(ay0, ay1) - by1, by0 - fmaxf(ay0, ay1)));
+                near |= !((dx * dx + dy * dy) * b.z > rc2);
+            }
+            if (!__syncthreads_or(near)) continue;
+        }
         __syncthreads();  // previous layer's shared data no longer in use
         const float *gd = t.lut_depths + (size_t)L.energy_id * t.lut_len;
         const float *gs = t.lut_sigmas + (size_t)L.energy_id * t.lut_len;

@@ -137,7 +137,7 @@ def _axis_wet_profile(rlsp, spacing, origin, src, iso, step_mm=1.0):
 
 
 def batch_plan(seed=0, shape=(160, 256, 256), spacing=(1.5, 1.5, 2.0), model=None, pitch_range=(4.0, 6.0),
-               max_beams=3, max_spots=12000):
+               max_beams=3, max_spots=12000, n_beams=None):
     """(IMPTDoseGrid, [IMPTBeam], target (centre, radius)) of one plan of the
     batched workload: a water-equivalent body ellipsoid (20 +- 40 HU) with 1-6
     random bone/lung/air ellipsoids (1000, -750, -1000 HU; semi-axes 5-40 mm)
@@ -151,25 +151,39 @@ def batch_plan(seed=0, shape=(160, 256, 256), spacing=(1.5, 1.5, 2.0), model=Non
     grid.origin = np.array([-nx * sx / 2.0, -ny * sy / 2.0, -nz * sz / 2.0])
     grid.spacing = np.array([sx, sy, sz])
     grid.size = np.array(shape)
-    z = (np.arange(nz) + 0.5) * sz + grid.origin[2]
-    y = (np.arange(ny) + 0.5) * sy + grid.origin[1]
-    x = (np.arange(nx) + 0.5) * sx + grid.origin[0]
-    Z, Y, X = np.meshgrid(z.astype(np.float32), y.astype(np.float32), x.astype(np.float32), indexing="ij")
+    z = ((np.arange(nz) + 0.5) * sz + grid.origin[2]).astype(np.float32)
+    y = ((np.arange(ny) + 0.5) * sy + grid.origin[1]).astype(np.float32)
+    x = ((np.arange(nx) + 0.5) * sx + grid.origin[0]).astype(np.float32)
     ext = np.array([nx * sx, ny * sy, nz * sz]) / 2.0
     body_ax = ext * rng.uniform(0.78, 0.92, size=3)
-    body = (X / body_ax[0]) ** 2 + (Y / body_ax[1]) ** 2 + (Z / body_ax[2]) ** 2 <= 1.0
+    body = ((x / body_ax[0]) ** 2)[None, None, :] + ((y / body_ax[1]) ** 2)[None, :, None] + \
+           ((z / body_ax[2]) ** 2)[:, None, None] <= 1.0
     hu = np.full(shape, -1000.0, np.float32)
-    hu[body] = (20.0 + 40.0 * rng.standard_normal(int(body.sum()))).astype(np.float32)
+    hu[body] = 20.0 + 40.0 * rng.standard_normal(int(body.sum()), dtype=np.float32)
+
+    def ellipsoid(c, a):
+        """(slices, mask) of an axis-aligned ellipsoid within its bounding box."""
+        sl, axes = [], []
+        for coords, cc, aa in ((z, c[2], a[2]), (y, c[1], a[1]), (x, c[0], a[0])):
+            lo = int(np.searchsorted(coords, cc - aa))
+            hi = int(np.searchsorted(coords, cc + aa, side="right"))
+            sl.append(slice(lo, max(lo, hi)))
+            axes.append(((coords[lo:max(lo, hi)] - cc) / aa) ** 2)
+        m = axes[0][:, None, None] + axes[1][None, :, None] + axes[2][None, None, :] <= 1.0
+        return tuple(sl), m
+
     for _ in range(int(rng.integers(1, 7))):
         c = rng.uniform(-0.5, 0.5, size=3) * body_ax
         a = rng.uniform(5.0, 40.0, size=3)
         val = float(rng.choice([1000.0, -750.0, -1000.0]))
-        m = ((X - c[0]) / a[0]) ** 2 + ((Y - c[1]) / a[1]) ** 2 + ((Z - c[2]) / a[2]) ** 2 <= 1.0
-        hu[m & body] = val
+        sl, m = ellipsoid(c, a)
+        sub = hu[sl]
+        sub[m & body[sl]] = val
     r_t = float(rng.uniform(20.0, 45.0))
     c_t = rng.uniform(-0.25, 0.25, size=3) * np.maximum(body_ax - r_t - 10.0, 0.0)
-    tgt = ((X - c_t[0]) ** 2 + (Y - c_t[1]) ** 2 + (Z - c_t[2]) ** 2) <= r_t ** 2
-    hu[tgt] = (20.0 + 40.0 * rng.standard_normal(int(tgt.sum()))).astype(np.float32)
+    sl, m = ellipsoid(c_t, np.array([r_t, r_t, r_t]))
+    sub = hu[sl]
+    sub[m] = 20.0 + 40.0 * rng.standard_normal(int(m.sum()), dtype=np.float32)
     grid.HU = hu
 
     if model is None:
@@ -179,7 +193,8 @@ def batch_plan(seed=0, shape=(160, 256, 256), spacing=(1.5, 1.5, 2.0), model=Non
     sad = (float(model.VSADX) + float(model.VSADY)) / 2.0
     beams = []
     total = 0
-    for _ in range(int(rng.integers(1, max_beams + 1))):
+    nb = int(rng.integers(1, max_beams + 1)) if n_beams is None else int(n_beams)
+    for _ in range(nb):
         ga = float(rng.uniform(0.0, 360.0))
         # source position for gantry ga (+180 inside the engine), couch 0
         g = np.deg2rad(np.float32((ga + 180.0) % 360.0))
@@ -204,7 +219,7 @@ def batch_plan(seed=0, shape=(160, 256, 256), spacing=(1.5, 1.5, 2.0), model=Non
             mu = rng.lognormal(0.0, 0.5, size=gx.size)
             rows.append(np.column_stack((gx, gy, mu, np.full(gx.size, e))))
         spots = np.array(np.vstack(rows), dtype=np.single)
-        if beams and total + spots.shape[0] > max_spots:
+        if beams and n_beams is None and total + spots.shape[0] > max_spots:
             break  # keep the plan within its spot budget
         total += spots.shape[0]
         beam = IMPTBeam()
