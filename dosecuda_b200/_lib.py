@@ -123,6 +123,41 @@ SIGNATURES = {
     "dc_photon_dose": (C.c_int, _VOL + [C.POINTER(PhotonModel), C.POINTER(ControlPoint), C.c_void_p]),
     "dc_photon_dose_dev": (C.c_int, _VOL + [C.POINTER(PhotonModel), C.POINTER(ControlPoint), C.c_void_p,
                                             C.c_void_p]),
+    "dc_photon_beam_create": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, _F3, _F3, C.POINTER(C.c_void_p)]),
+    "dc_photon_beam_destroy": (C.c_int, [C.c_void_p]),
+    "dc_photon_beam_set_density": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "dc_photon_beam_terma": (C.c_int, [C.c_void_p, C.POINTER(PhotonModel), C.POINTER(ControlPoint), C.c_void_p,
+                                       C.c_void_p]),
+    "dc_photon_beam_dose": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "dc_photon_beam_probe_select": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.c_void_p]),
+    "dc_photon_beam_probe_list": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_int), C.c_void_p,
+                                            C.c_int]),
+    "dc_photon_beam_probe": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
+    "dc_gamma": (C.c_int, [C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_int, _F3, C.c_void_p, C.c_void_p, C.c_longlong,
+                           C.c_float, C.c_float, C.c_float, C.c_float, C.c_void_p, C.c_void_p]),
+    "dc_net_packed_fragments": (C.c_longlong, [C.c_int, C.c_int, C.c_int]),
+    "dc_net_pack_weights": (C.c_int, [C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p,
+                                      C.c_void_p]),
+    "dc_net_conv": (C.c_int, [C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p,
+                              C.c_longlong, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "dc_net_conv_up": (C.c_int, [C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p,
+                                 C.c_longlong, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "dc_net_wgrad": (C.c_int, [C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
+                               C.c_int, C.c_void_p, C.c_void_p]),
+    "dc_net_norm_finalize": (C.c_int, [C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_longlong, C.c_void_p, C.c_void_p,
+                                       C.c_float, C.c_void_p, C.c_void_p]),
+    "dc_net_norm_act": (C.c_int, [C.c_int, C.c_void_p, C.c_int, C.c_longlong, C.c_int, C.c_void_p, C.c_float,
+                                  C.c_void_p, C.c_void_p]),
+    "dc_net_norm_act_bwd": (C.c_int, [C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_longlong, C.c_int, C.c_void_p,
+                                      C.c_void_p, C.c_float, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                      C.c_void_p]),
+    "dc_net_pack_input": (C.c_int, [C.c_int, C.c_void_p, C.c_void_p, C.c_longlong, C.c_float, C.c_void_p,
+                                    C.c_void_p]),
+    "dc_net_head": (C.c_int, [C.c_int, C.c_void_p, C.c_longlong, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
+                              C.c_float, C.c_float, C.c_void_p, C.c_void_p]),
+    "dc_net_head_loss_bwd": (C.c_int, [C.c_int, C.c_void_p, C.c_longlong, C.c_int, C.c_void_p, C.c_void_p,
+                                       C.c_void_p, C.c_float, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                       C.c_void_p]),
 }
 
 _lib = None

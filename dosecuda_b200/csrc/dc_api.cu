@@ -23,24 +23,6 @@ using namespace dc;
 
 namespace {
 
-template <class F>
-int guarded(F &&fn) {
-    try {
-        fn();
-        set_last_error("");
-        return DC_OK;
-    } catch (const Error &e) {
-        set_last_error(e.what());
-        return e.code;
-    } catch (const std::bad_alloc &) {
-        set_last_error("Not enough host memory");
-        return DC_ERR_MEMORY;
-    } catch (const std::exception &e) {
-        set_last_error(e.what());
-        return DC_ERR_CUDA;
-    }
-}
-
 void need(bool ok, const std::string &msg) {
     if (!ok) throw Error(DC_ERR_VALUE, msg);
 }

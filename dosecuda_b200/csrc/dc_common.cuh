@@ -31,7 +31,7 @@ struct Grid {
     int nx, ny, nz;
     float sx, sy, sz;           // spacing, mm
     float inv_sx, inv_sy, inv_sz;  // 1/spacing (IEEE-rounded, as 1.0f/sp on device)
-    long long n() const { return (long long)nx * ny * nz; }
+    __host__ __device__ long long n() const { return (long long)nx * ny * nz; }
 };
 
 // Beam geometry: isocentre (relative to the volume origin), source position
@@ -93,7 +93,7 @@ __device__ __forceinline__ float distance_to_source(const Frame &f, float3 p) {
 // Image -> head frame: couch, then gantry, then (photons) collimator, then the
 // DICOM nozzle axis swap (CudaClasses.cu:65-95, IMRTClasses.cu:41-79).
 template <bool kCollimator>
-__device__ __forceinline__ float3 image_to_head(const Frame &f, float3 p) {
+__host__ __device__ __forceinline__ float3 image_to_head(const Frame &f, float3 p) {
     float s = -f.sta, c = f.cta;
     const float xt = p.x * c + p.z * s;
     const float yt = p.y;
@@ -117,7 +117,7 @@ __device__ __forceinline__ float3 image_to_head(const Frame &f, float3 p) {
 // Head -> image frame, the inverse sequence (CudaClasses.cu:97-126,
 // IMRTClasses.cu:81-118).
 template <bool kCollimator>
-__device__ __forceinline__ float3 head_to_image(const Frame &f, float3 h) {
+__host__ __device__ __forceinline__ float3 head_to_image(const Frame &f, float3 h) {
     float x = -h.x;
     float y = h.z;
     float z = h.y;

@@ -76,10 +76,13 @@ __device__ __forceinline__ float head_transmission(const PhotonParams &P, float3
 // CCCS mask (dose 0 where TERMA <= 0.01, IMRTClasses.cu:270-273): masked
 // voxels get their zero dose here, the others are appended to `active`
 // (warp-aggregated), so the CCCS runs on full warps of active voxels only.
+// dose (or null) receives the zero of masked voxels; terma_out (or null) a
+// linear copy of the TERMA volume.
 __global__ void __launch_bounds__(128) terma_kernel(Grid g, Frame f, PhotonParams P, const float *__restrict__ wet,
                                                     cudaTextureObject_t dens_tex, cudaSurfaceObject_t td_surf,
                                                     float *__restrict__ electron, float *__restrict__ dose,
-                                                    int *__restrict__ active, unsigned *__restrict__ n_active) {
+                                                    float *__restrict__ terma_out, int *__restrict__ active,
+                                                    unsigned *__restrict__ n_active) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
     const int k = blockIdx.z;
@@ -128,9 +131,10 @@ __global__ void __launch_bounds__(128) terma_kernel(Grid g, Frame f, PhotonParam
     const float rho = tex3D<float>(dens_tex, (float)i + 0.5f, (float)j + 0.5f, (float)k + 0.5f);
     surf3Dwrite(make_float2(T, rho), td_surf, i * (int)sizeof(float2), j, k);
     electron[v] = P.esw * (0.4f + (0.3f * ratio)) * elec * tp;
+    if (terma_out) terma_out[v] = T;
 
     const bool act = !(T <= 0.01f);
-    if (!act) dose[v] = 0.0f;
+    if (!act && dose) dose[v] = 0.0f;
     const unsigned live = __activemask();
     const unsigned bal = __ballot_sync(live, act);
     if (act) {
@@ -196,6 +200,42 @@ __global__ void __launch_bounds__(128) cccs_kernel(Grid g, Frame f, CccsCones C,
         float dose_value = cccs_voxel(g, f, C, sp_cm, s_dir, s_rl10, td_tex, p);
         dose_value += __ldg(electron + v);
         dose[v] = (!isnan(dose_value) && dose_value >= 0.0f) ? dose_scale * dose_value : 0.0f;
+    }
+}
+
+// CCCS at an arbitrary list of voxels (the surrogate's probe): the same
+// per-voxel sum as cccs_kernel, with the mask taken from the TERMA texel.
+__global__ void __launch_bounds__(128) cccs_points_kernel(Grid g, Frame f, CccsCones C, float sp_cm, float dose_scale,
+                                                          const float4 *__restrict__ dirs, cudaTextureObject_t td_tex,
+                                                          const float *__restrict__ electron,
+                                                          const int *__restrict__ voxels, int n,
+                                                          float *__restrict__ out) {
+    __shared__ float4 s_dir[kMaxCones * 12];
+    __shared__ float s_rl10[kMaxConeSteps];
+    const int tid = threadIdx.x;
+    for (int q = tid; q < C.n_cones * 12; q += blockDim.x) s_dir[q] = dirs[q];
+    for (int q = tid; q < C.total_steps; q += blockDim.x) s_rl10[q] = C.rl10[q];
+    __syncthreads();
+    const int plane = g.nx * g.ny;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+        const int v = __ldg(voxels + t);
+        if (v < 0 || (long long)v >= g.n()) {  // not a voxel of the grid
+            out[t] = 0.0f;
+            continue;
+        }
+        const int k = v / plane;
+        const int rem = v - k * plane;
+        const int j = rem / g.nx;
+        const int i = rem - j * g.nx;
+        const float T = tex3D<float2>(td_tex, (float)i + 0.5f, (float)j + 0.5f, (float)k + 0.5f).x;
+        float r = 0.0f;
+        if (!(T <= 0.01f)) {
+            const float3 p = voxel_xyz(g, f, i, j, k);
+            float dose_value = cccs_voxel(g, f, C, sp_cm, s_dir, s_rl10, td_tex, p);
+            dose_value += __ldg(electron + v);
+            r = (!isnan(dose_value) && dose_value >= 0.0f) ? dose_scale * dose_value : 0.0f;
+        }
+        out[t] = r;
     }
 }
 
@@ -338,47 +378,68 @@ void build_photon_params(const dc_photon_model &m, const dc_control_point &cp, f
     C.total_steps = off;
 }
 
+static unsigned cccs_blocks(const DeviceContext &ctx, long long work) {
+    // persistent grid: as many resident CTAs as fit on every SM
+    int sms = 0, per_sm = 0;
+    DC_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx.device));
+    DC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cccs_kernel, 128, 0));
+    const long long want = (work + 127) / 128;
+    return (unsigned)std::max(1LL, std::min<long long>(want, (long long)sms * std::max(per_sm, 1)));
+}
+
+void enqueue_terma(DeviceContext &ctx, const Grid &g, const Frame &f, const PhotonParams &P, const CccsCones &C,
+                   const PhotonWork &w, float *dose_dev, float *terma_out, cudaStream_t s) {
+    if (g.n() > 0x7fffffffLL) throw Error(DC_ERR_VALUE, "photon volumes are limited to 2^31 - 1 voxels.");
+    launch_wet_march(ctx, g, f, w.dens_tex, w.wet, s);
+    DC_CUDA(cudaMemsetAsync(w.n_active, 0, sizeof(unsigned), s));
+    {
+        KernelTimer kt(ctx, "terma", s);
+        terma_kernel<<<vol_grid(g), dim3(32, 4, 1), 0, s>>>(g, f, P, w.wet, w.dens_tex, w.td_surf, w.electron,
+                                                            dose_dev, terma_out, w.active, w.n_active);
+        check_launch("terma_kernel");
+    }
+    cone_dirs_kernel<<<1, kMaxCones * 12, 0, s>>>(f, C, w.dirs);
+    check_launch("cone_dirs_kernel");
+}
+
+void enqueue_cccs(DeviceContext &ctx, const Grid &g, const Frame &f, const CccsCones &C, const PhotonWork &w,
+                  float dose_scale, float *dose_dev, cudaStream_t s) {
+    KernelTimer kt(ctx, "cccs", s);
+    cccs_kernel<<<cccs_blocks(ctx, g.n()), 128, 0, s>>>(g, f, C, g.sx / 10.0f, dose_scale, w.dirs, w.td_tex,
+                                                        w.electron, w.active, w.n_active, dose_dev);
+    check_launch("cccs_kernel");
+}
+
+void enqueue_cccs_points(DeviceContext &ctx, const Grid &g, const Frame &f, const CccsCones &C, const PhotonWork &w,
+                         float dose_scale, const int *voxels, int n, float *out, cudaStream_t s) {
+    if (n <= 0) return;
+    KernelTimer kt(ctx, "cccs_points", s);
+    cccs_points_kernel<<<cccs_blocks(ctx, n), 128, 0, s>>>(g, f, C, g.sx / 10.0f, dose_scale, w.dirs, w.td_tex,
+                                                           w.electron, voxels, n, out);
+    check_launch("cccs_points_kernel");
+}
+
 void run_photon_pipeline(DeviceContext &ctx, const Grid &g, const Frame &f, const PhotonParams &P,
                          const CccsCones &C, float dose_scale, float *dose_dev, cudaStream_t s) {
     const long long n = g.n();
+    if (n > 0x7fffffffLL) throw Error(DC_ERR_VALUE, "photon volumes are limited to 2^31 - 1 voxels.");
+    PhotonWork w;
     // The density volume is already in ctx.density; border AIR_DENSITY
     // (IMRTClasses.cu:394).
-    cudaTextureObject_t dens_tex = ctx.density.texture(kAirDensity);
+    w.dens_tex = ctx.density.texture(kAirDensity);
     // (TERMA, density) volume: TERMA border 0 (IMRTClasses.cu:399), density
     // border AIR_DENSITY (:394).
     ctx.terma.ensure(g.nx, g.ny, g.nz, true, 2);
-    cudaTextureObject_t td_tex = ctx.terma.texture(0.0f, kAirDensity);
-
-    if (n > 0x7fffffffLL) throw Error(DC_ERR_VALUE, "photon volumes are limited to 2^31 - 1 voxels.");
-    float *wet = static_cast<float *>(ctx.wet_raw.ensure((size_t)n * sizeof(float)));
-    float *elec = static_cast<float *>(ctx.electron.ensure((size_t)n * sizeof(float)));
-    float4 *dirs = static_cast<float4 *>(ctx.small.ensure(kMaxCones * 12 * sizeof(float4)));
+    w.td_tex = ctx.terma.texture(0.0f, kAirDensity);
+    w.td_surf = ctx.terma.surf;
+    w.wet = static_cast<float *>(ctx.wet_raw.ensure((size_t)n * sizeof(float)));
+    w.electron = static_cast<float *>(ctx.electron.ensure((size_t)n * sizeof(float)));
+    w.dirs = static_cast<float4 *>(ctx.small.ensure(kMaxCones * 12 * sizeof(float4)));
     char *act = static_cast<char *>(ctx.active.ensure(256 + (size_t)n * sizeof(int)));
-    unsigned *n_active = reinterpret_cast<unsigned *>(act);
-    int *active = reinterpret_cast<int *>(act + 256);
-
-    launch_wet_march(ctx, g, f, dens_tex, wet, s);
-    DC_CUDA(cudaMemsetAsync(n_active, 0, sizeof(unsigned), s));
-    {
-        KernelTimer kt(ctx, "terma", s);
-        terma_kernel<<<vol_grid(g), dim3(32, 4, 1), 0, s>>>(g, f, P, wet, dens_tex, ctx.terma.surf, elec, dose_dev,
-                                                            active, n_active);
-        check_launch("terma_kernel");
-    }
-    cone_dirs_kernel<<<1, kMaxCones * 12, 0, s>>>(f, C, dirs);
-    check_launch("cone_dirs_kernel");
-    {
-        // persistent grid: as many resident CTAs as fit on every SM
-        int sms = 0, per_sm = 0;
-        DC_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx.device));
-        DC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cccs_kernel, 128, 0));
-        const long long want = (n + 127) / 128;
-        const unsigned blocks = (unsigned)std::max(1LL, std::min<long long>(want, (long long)sms * std::max(per_sm, 1)));
-        KernelTimer kt(ctx, "cccs", s);
-        cccs_kernel<<<blocks, 128, 0, s>>>(g, f, C, g.sx / 10.0f, dose_scale, dirs, td_tex, elec, active, n_active,
-                                           dose_dev);
-        check_launch("cccs_kernel");
-    }
+    w.n_active = reinterpret_cast<unsigned *>(act);
+    w.active = reinterpret_cast<int *>(act + 256);
+    enqueue_terma(ctx, g, f, P, C, w, dose_dev, nullptr, s);
+    enqueue_cccs(ctx, g, f, C, w, dose_scale, dose_dev, s);
 }
 
 }  // namespace dc

@@ -35,6 +35,29 @@ struct CccsCones {
 void build_photon_params(const dc_photon_model &m, const dc_control_point &cp, float spacing_cm,
                          PhotonParams &P, CccsCones &C);
 
+// Device work buffers of one photon calculation.
+struct PhotonWork {
+    float *wet = nullptr;          // radiological depth, n floats
+    float *electron = nullptr;     // electron contamination, n floats
+    unsigned *n_active = nullptr;  // number of CCCS voxels (device counter)
+    int *active = nullptr;         // CCCS voxel list, n ints
+    float4 *dirs = nullptr;        // kMaxCones*12 image-frame cone directions
+    cudaTextureObject_t dens_tex = 0;  // density, border AIR_DENSITY
+    cudaSurfaceObject_t td_surf = 0;   // (TERMA, density) float2 array
+    cudaTextureObject_t td_tex = 0;    // its texture, border (0, AIR_DENSITY)
+};
+
+// Ray trace + TERMA + cone directions.  dose_dev (or null) receives the zero
+// of every masked voxel, terma_out (or null) a linear TERMA copy.
+void enqueue_terma(DeviceContext &ctx, const Grid &g, const Frame &f, const PhotonParams &P, const CccsCones &C,
+                   const PhotonWork &w, float *dose_dev, float *terma_out, cudaStream_t s);
+// CCCS of every active voxel listed by the last enqueue_terma.
+void enqueue_cccs(DeviceContext &ctx, const Grid &g, const Frame &f, const CccsCones &C, const PhotonWork &w,
+                  float dose_scale, float *dose_dev, cudaStream_t s);
+// CCCS at n listed voxels into out[0..n).
+void enqueue_cccs_points(DeviceContext &ctx, const Grid &g, const Frame &f, const CccsCones &C, const PhotonWork &w,
+                         float dose_scale, const int *voxels, int n, float *out, cudaStream_t s);
+
 // Enqueues ray trace -> TERMA -> CCCS for one control point on stream s.
 // The density volume must already be in ctx.density; dose_dev: device output.
 void run_photon_pipeline(DeviceContext &ctx, const Grid &g, const Frame &f, const PhotonParams &P,

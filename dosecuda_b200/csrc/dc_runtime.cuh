@@ -14,8 +14,11 @@
 
 #include <cuda_runtime.h>
 
+#include "../../include/dosecuda.h"
+
 #include <map>
 #include <mutex>
+#include <new>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -36,6 +39,27 @@ inline void cuda_check(cudaError_t e, const char *what) {
 #define DC_CUDA(call) ::dc::cuda_check((call), #call)
 
 void set_last_error(const std::string &msg);
+
+// Runs fn and maps what it throws onto the C-ABI status codes (the message
+// goes to dc_last_error): Error -> its code, std::bad_alloc ->
+// DC_ERR_MEMORY, anything else -> DC_ERR_CUDA.
+template <class F>
+int guarded(F &&fn) {
+    try {
+        fn();
+        set_last_error("");
+        return DC_OK;
+    } catch (const Error &e) {
+        set_last_error(e.what());
+        return e.code;
+    } catch (const std::bad_alloc &) {
+        set_last_error("Not enough host memory");
+        return DC_ERR_MEMORY;
+    } catch (const std::exception &e) {
+        set_last_error(e.what());
+        return DC_ERR_CUDA;
+    }
+}
 
 // Grow-only device allocation.
 struct DeviceBuffer {

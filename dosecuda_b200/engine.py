@@ -388,3 +388,119 @@ class ProtonBatch:
             self.close()
         except Exception:
             pass
+
+
+class PhotonBeam:
+    """A photon calculation kept on one device for a fixed grid (C ABI
+    ``dc_photon_beam_*``): one ray trace + TERMA pass per control point, after
+    which the full CCCS dose and the CCCS dose at any list of voxels (a sparse
+    probe) come from the same TERMA.  Results equal ``photon_dose``."""
+
+    def __init__(self, grid, shape, device="cuda"):
+        dev = torch.device(device)
+        if dev.index is None:
+            dev = torch.device("cuda", torch.cuda.current_device())
+        self.device = dev
+        self.shape = tuple(int(s) for s in shape)
+        self.spacing = np.asarray(grid.spacing, np.float32).reshape(-1)
+        if self.spacing.size == 1:
+            self.spacing = np.repeat(self.spacing, 3)
+        self._grid = grid
+        self._h = C.c_void_p()
+        nz, ny, nx = self.shape
+        with torch.cuda.device(dev):
+            _lib.raise_for(_lib.load().dc_photon_beam_create(dev.index, nz, ny, nx, _spacing(grid),
+                                                              _lib.f3(grid.origin), C.byref(self._h)))
+        self.n_probe = 0
+        self._views = None
+
+    def close(self):
+        if self._h:
+            _lib.load().dc_photon_beam_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _s(self, stream):
+        s = stream if stream is not None else torch.cuda.current_stream(self.device)
+        return C.c_void_p(s.cuda_stream)
+
+    def set_density(self, density: torch.Tensor, stream=None):
+        _check_volume(density, "density")
+        if tuple(density.shape) != self.shape:
+            raise ValueError("'density' must have the beam's shape %s." % (self.shape,))
+        _lib.raise_for(_lib.load().dc_photon_beam_set_density(self._h, C.c_void_p(density.data_ptr()),
+                                                               self._s(stream)))
+
+    def terma(self, model, cp, out=None, views=None, stream=None) -> torch.Tensor | None:
+        """Ray trace + TERMA of control point ``cp``; returns the TERMA volume
+        when ``out`` is given (or ``out=True`` to allocate it)."""
+        mv, cv = views if views is not None else (PhotonModelView(model), ControlPointView(cp))
+        self._views = (mv, cv)  # keep the packed arrays alive while the call is in flight
+        if out is True:
+            out = torch.empty(self.shape, dtype=torch.float32, device=self.device)
+        ptr = C.c_void_p(out.data_ptr()) if out is not None else None
+        _lib.raise_for(_lib.load().dc_photon_beam_terma(self._h, C.byref(mv.struct), C.byref(cv.struct), ptr,
+                                                         self._s(stream)))
+        self.n_probe = 0
+        return out
+
+    def dose(self, out=None, stream=None) -> torch.Tensor:
+        if out is None:
+            out = torch.empty(self.shape, dtype=torch.float32, device=self.device)
+        _lib.raise_for(_lib.load().dc_photon_beam_dose(self._h, C.c_void_p(out.data_ptr()), self._s(stream)))
+        return out
+
+    def select_probe(self, stream=None) -> int:
+        n = C.c_int()
+        _lib.raise_for(_lib.load().dc_photon_beam_probe_select(self._h, C.byref(n), self._s(stream)))
+        self.n_probe = n.value
+        return self.n_probe
+
+    def probe_voxels(self) -> tuple[int, int, np.ndarray]:
+        """(device pointer, count, host copy) of the selected probe voxels."""
+        p, n = C.c_void_p(), C.c_int()
+        host = np.empty(max(self.n_probe, 1), np.int32)
+        _lib.raise_for(_lib.load().dc_photon_beam_probe_list(self._h, C.byref(p), C.byref(n),
+                                                              host.ctypes.data_as(C.c_void_p), host.size))
+        return p.value or 0, n.value, host[:n.value]
+
+    def probe(self, voxels: torch.Tensor | None = None, out=None, stream=None) -> torch.Tensor:
+        """CCCS dose at ``voxels`` (int32 flat indices) or at the selected probe."""
+        n = int(voxels.numel()) if voxels is not None else self.n_probe
+        if out is None:
+            out = torch.empty(max(n, 1), dtype=torch.float32, device=self.device)[:n]
+        vp = C.c_void_p(voxels.data_ptr()) if voxels is not None else None
+        _lib.raise_for(_lib.load().dc_photon_beam_probe(self._h, vp, n, C.c_void_p(out.data_ptr()),
+                                                         self._s(stream)))
+        return out
+
+
+def gamma_counts(eval_dose: torch.Tensor, spacing, ref: torch.Tensor, voxels: torch.Tensor | int | None = None,
+                 n: int | None = None, dose_norm: float = 0.0, dta_mm: float = 2.0, dd_frac: float = 0.02,
+                 cutoff_frac: float = 0.1, counts: torch.Tensor | None = None, stream=None) -> torch.Tensor:
+    """Gamma index of ``eval_dose`` against reference doses on the device
+    (C ABI ``dc_gamma``): ``ref`` is a volume (``voxels`` None) or the doses at
+    the listed voxels (a tensor of int32 indices, or a raw device pointer with
+    ``n``).  Returns the int32 device tensor [evaluated, passed, -, -]."""
+    _check_volume(eval_dose, "eval_dose")
+    nz, ny, nx = eval_dose.shape
+    if counts is None:
+        counts = torch.empty(4, dtype=torch.int32, device=eval_dose.device)
+    sp = np.asarray(spacing, np.float32).reshape(-1)
+    sp3 = _lib.f3(sp if sp.size == 3 else np.repeat(sp, 3))
+    if voxels is None:
+        vp, count = None, nz * ny * nx
+    elif isinstance(voxels, torch.Tensor):
+        vp, count = C.c_void_p(voxels.data_ptr()), int(voxels.numel())
+    else:
+        vp, count = C.c_void_p(int(voxels)), int(n)
+    _lib.raise_for(_lib.load().dc_gamma(
+        eval_dose.device.index, C.c_void_p(eval_dose.data_ptr()), nz, ny, nx, sp3, vp,
+        C.c_void_p(ref.data_ptr()), count, float(dose_norm), float(dta_mm), float(dd_frac), float(cutoff_frac),
+        C.c_void_p(counts.data_ptr()), _stream(eval_dose, stream)))
+    return counts

@@ -289,6 +289,119 @@ int dc_photon_dose_dev(int gpu_id,
                        const dc_photon_model *model, const dc_control_point *cp,
                        float *dose_out_dev, void *stream);
 
+/* ------------------------------------------------------------------ */
+/* Photon beam kept on the device (surrogate path).  No counterpart in  */
+/* the reference: it splits dc_photon_dose into its TERMA pass and its  */
+/* CCCS pass so that one TERMA serves the surrogate's input, a sparse   */
+/* CCCS probe and, on rejection, the full CCCS.  Same kernels and       */
+/* results as dc_photon_dose.  All volume pointers are device pointers. */
+/* ------------------------------------------------------------------ */
+typedef struct dc_photon_beam dc_photon_beam;
+
+int dc_photon_beam_create(int gpu_id, int nz, int ny, int nx, const float spacing[3], const float origin[3],
+                          dc_photon_beam **out);
+int dc_photon_beam_destroy(dc_photon_beam *beam);
+/* Copies the relative-density volume (device, (nz,ny,nx) float32). */
+int dc_photon_beam_set_density(dc_photon_beam *beam, const float *density_dev, void *stream);
+/* Ray trace + TERMA of one control point; terma_out_dev (or NULL)
+ * receives the TERMA volume. */
+int dc_photon_beam_terma(dc_photon_beam *beam, const dc_photon_model *model, const dc_control_point *cp,
+                         float *terma_out_dev, void *stream);
+/* Full CCCS dose of the last TERMA (as dc_photon_dose_dev). */
+int dc_photon_beam_dose(dc_photon_beam *beam, float *dose_out_dev, void *stream);
+/* Selects the probe voxels of the last TERMA's control point: rays from
+ * the source through the open field's centre, half-field and edge
+ * positions, and lateral profiles at three depths.  Synchronous. */
+int dc_photon_beam_probe_select(dc_photon_beam *beam, int *n_out, void *stream);
+/* The selected list: device pointer and count, and optionally a host copy
+ * of the first `cap` indices. */
+int dc_photon_beam_probe_list(const dc_photon_beam *beam, const int **voxels_dev, int *n, int *voxels_host, int cap);
+/* CCCS dose at n listed voxels (voxels_dev NULL: the selected list). */
+int dc_photon_beam_probe(dc_photon_beam *beam, const int *voxels_dev, int n, float *dose_out_dev, void *stream);
+
+/* Gamma index of the evaluated volume eval (nz,ny,nx) against reference
+ * doses: ref[i] at voxel voxels[i] (i < n), or, with voxels NULL, the
+ * reference volume ref.  Global dose criterion dd_frac*dose_norm (dose_norm
+ * <= 0: the maximum of eval), distance dta_mm, reference points below
+ * cutoff_frac*dose_norm skipped.  counts_dev[4]: [0] evaluated points,
+ * [1] points with gamma <= 1, [2] scratch (all overwritten). */
+int dc_gamma(int gpu_id, const float *eval_dev, int nz, int ny, int nx, const float spacing[3], const int *voxels_dev,
+             const float *ref_dev, long long n, float dose_norm, float dta_mm, float dd_frac, float cutoff_frac,
+             int *counts_dev, void *stream);
+
+/* ------------------------------------------------------------------ */
+/* Surrogate network building blocks (photon dose from TERMA+density). */
+/* No counterpart in the reference, which has no learned model.         */
+/* All pointers are device pointers on gpu_id; work is enqueued on      */
+/* `stream` (NULL: legacy default stream) and nothing is synchronised.  */
+/* Activations are bf16 (uint16 storage), channels-last (n,d,h,w,c).    */
+/* Master weights are fp32:                                              */
+/*   3x3x3 and 2x2x2-stride-2 convolutions: [taps][cin][cout],           */
+/*     tap = (dz*k + dy)*k + dx;                                         */
+/*   transposed 2x2x2 convolution: [8][cout][cin].                       */
+/* Supported channel pairs: 3x3x3 8->16, 16->16, 32->32, 64->64,         */
+/* 128->128; 2x2x2 stride 2 16->32, 32->64, 64->128; transposed          */
+/* 32->16, 64->32, 128->64 (and their backward passes).                  */
+/* ------------------------------------------------------------------ */
+#define DC_NET_CONV3 0 /* 3x3x3, stride 1, zero padding 1 (same grid)  */
+#define DC_NET_DOWN2 1 /* 2x2x2, stride 2 (grid halves)                 */
+
+/* Number of 8-byte fragments of a packed weight set: ceil(taps*k/16) *
+ * (n/8) * 32, where k is the reduction and n the output channel count. */
+long long dc_net_packed_fragments(int taps, int k_per_tap, int n);
+
+/* Packs master weights m[taps][a][b] into mma fragment order for a GEMM
+ * with output channels n = (trans ? a : b) and reduction k = (trans ? b :
+ * a) per tap; flip reverses the tap order (the 3x3x3 backward-data pass). */
+int dc_net_pack_weights(int gpu_id, const float *master_dev, int taps, int a, int b, int flip, int trans,
+                        void *packed_dev, void *stream);
+
+/* Gather convolution y = conv(x) (mode DC_NET_CONV3 or DC_NET_DOWN2),
+ * x: (n,d,h,w,cin), y on the output grid; wpk_frags: size of the packed
+ * weights (must equal dc_net_packed_fragments(taps, cin, cout)).  stats (or
+ * NULL): [n][cout][2] sum and sum of squares of the stored bf16 outputs
+ * (overwritten). */
+int dc_net_conv(int gpu_id, int mode, const void *x_dev, int n, int d, int h, int w, int cin, const void *wpk_dev,
+                long long wpk_frags, int cout, void *y_dev, double *stats_dev, void *stream);
+
+/* Transposed 2x2x2 stride-2 convolution y = up(x) + addend, x on the
+ * coarse grid (n,d,h,w,cin), y on (n,2d,2h,2w,cout); addend may be NULL or
+ * alias y. */
+int dc_net_conv_up(int gpu_id, const void *x_dev, int n, int d, int h, int w, int cin, const void *wpk_dev,
+                   long long wpk_frags, int cout, const void *addend_dev, void *y_dev, void *stream);
+
+/* Weight gradient G[taps][ca][cb] = sum_o P[g(o,t)][a] Q[o][b] over the Q
+ * grid (n,d,h,w,cb); P is on the same grid (DC_NET_CONV3, 27 taps) or on
+ * the doubled grid (DC_NET_DOWN2, 8 taps).  grad is overwritten. */
+int dc_net_wgrad(int gpu_id, int mode, const void *p_dev, const void *q_dev, int n, int d, int h, int w, int ca,
+                 int cb, float *grad_dev, void *stream);
+
+/* Instance norm: coef[n][c] = (gamma*rstd, beta - mean*gamma*rstd, mean,
+ * rstd) from the statistics of dc_net_conv over `count` voxels. */
+int dc_net_norm_finalize(int gpu_id, const double *stats_dev, int n, int c, long long count, const float *gamma_dev,
+                         const float *beta_dev, float eps, float *coef_dev, void *stream);
+/* a = leaky_relu(coef.x*y + coef.y, slope). */
+int dc_net_norm_act(int gpu_id, const void *y_dev, int n, long long vox, int c, const float *coef_dev, float slope,
+                    void *a_dev, void *stream);
+/* Backward of norm+activation: dy from da, and dgamma/dbeta (overwritten);
+ * red: [n][c][2] double scratch. */
+int dc_net_norm_act_bwd(int gpu_id, const void *y_dev, const void *da_dev, int n, long long vox, int c,
+                        const float *coef_dev, const float *gamma_dev, float slope, double *red_dev, void *dy_dev,
+                        float *dgamma_dev, float *dbeta_dev, void *stream);
+
+/* Network input: x8[v] = (terma*terma_scale, density, 0 x 6). */
+int dc_net_pack_input(int gpu_id, const float *terma_dev, const float *density_dev, long long vox, float terma_scale,
+                      void *x8_dev, void *stream);
+/* Output head (16 channels -> 1): out = mask > mask_thr ?
+ * scale*(w.g + bias) : 0. */
+int dc_net_head(int gpu_id, const void *g_dev, long long vox, int c, const float *w_dev, const float *bias_dev,
+                const float *mask_dev, float mask_thr, float scale, float *out_dev, void *stream);
+/* Squared-error loss over voxels with target >= 0, times inv_count, and
+ * its gradients: dg (16 channels), dw, dbias, loss (all overwritten). */
+int dc_net_head_loss_bwd(int gpu_id, const void *g_dev, long long vox, int c, const float *w_dev,
+                         const float *pred_dev, const float *target_dev, float inv_count, double *loss_dev,
+                         void *dg_dev, float *dw_dev, float *dbias_dev, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,327 @@
+"""Surrogate-network kernels (dc_net_*) against a float64 CPU torch
+reference: each convolution form forward, backward-data and backward-weight,
+instance norm + LeakyReLU forward/backward, the head and loss, and the whole
+encoder-decoder's forward pass and parameter gradients.
+
+Inputs and weights are bf16-representable, so single-kernel differences come
+only from fp32 accumulation and the final bf16 rounding of the output."""
+import numpy as np
+import pytest
+import torch
+import torch.nn.functional as F
+
+import netref as R
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def ops():
+    from dosecuda_b200.surrogate import NetOps
+    return NetOps("cuda")
+
+
+def _rand(shape, seed, scale=1.0):
+    g = torch.Generator().manual_seed(seed)
+    return (torch.randn(shape, generator=g, dtype=torch.float64) * scale)
+
+
+def _act(shape, seed):
+    """bf16 device activation and its float64 CPU copy (NDHWC)."""
+    x = R.bf16(_rand(shape, seed))
+    return x.to(torch.bfloat16).cuda(), x
+
+
+def _close(got, ref, rtol=1e-2, atol_frac=2e-3):
+    got = got.detach().double().cpu()
+    ref = ref.double()
+    atol = atol_frac * float(ref.abs().max())
+    err = (got - ref).abs()
+    bad = err > atol + rtol * ref.abs()
+    assert not bool(bad.any()), "max err %.3e (max |ref| %.3e), %d bad of %d" % (
+        float(err.max()), float(ref.abs().max()), int(bad.sum()), ref.numel())
+
+
+CONV3_PAIRS = [(8, 16), (16, 16), (32, 32), (64, 64), (128, 128)]
+DOWN_PAIRS = [(16, 32), (32, 64), (64, 128)]
+UP_PAIRS = [(32, 16), (64, 32), (128, 64)]
+
+
+@pytest.mark.parametrize("cin,cout", CONV3_PAIRS)
+def test_conv3_forward_and_stats(ops, cin, cout):
+    x, xr = _act((2, 5, 11, 20, cin), 1)
+    w = R.bf16(_rand((27, cin, cout), 2, 1.0 / np.sqrt(27 * cin)))
+    stats = torch.empty((2, cout, 2), dtype=torch.float64, device="cuda")
+    y = ops.conv(0, x, ops.pack(w.float().cuda()), cout, stats=stats)
+    ref = R.ndhwc(F.conv3d(R.ncdhw(xr), R.conv3_weight(w), padding=1))
+    _close(y, ref)
+    yd = y.double().cpu()
+    s1 = yd.sum(dim=(1, 2, 3))
+    s2 = (yd * yd).sum(dim=(1, 2, 3))
+    torch.testing.assert_close(stats[..., 0].cpu(), s1, rtol=1e-4, atol=1e-3)
+    torch.testing.assert_close(stats[..., 1].cpu(), s2, rtol=1e-4, atol=1e-3)
+
+
+@pytest.mark.parametrize("cin,cout", CONV3_PAIRS)
+def test_conv3_backward(ops, cin, cout):
+    x, xr = _act((1, 6, 9, 18, cin), 3)
+    dy, dyr = _act((1, 6, 9, 18, cout), 4)
+    w = R.bf16(_rand((27, cin, cout), 5, 1.0 / np.sqrt(27 * cin)))
+    wt = R.conv3_weight(w)
+    if cin >= 16:  # (the network never needs the gradient of its 8-channel input)
+        # backward-data: the 3x3x3 gather with flipped, transposed weights
+        dx = ops.conv(0, dy, ops.pack(w.float().cuda(), 1, 1), cin)
+        ref_dx = torch.nn.grad.conv3d_input(R.ncdhw(xr).shape, wt, R.ncdhw(dyr), padding=1)
+        _close(dx, R.ndhwc(ref_dx))
+    # backward-weight
+    g = ops.wgrad(0, x, dy, cin)
+    ref_w = torch.nn.grad.conv3d_weight(R.ncdhw(xr), wt.shape, R.ncdhw(dyr), padding=1)  # (cout, cin, 3,3,3)
+    ref_g = ref_w.permute(2, 3, 4, 1, 0).reshape(27, cin, cout)
+    _close(g, ref_g, rtol=1e-4, atol_frac=1e-4)
+
+
+@pytest.mark.parametrize("cin,cout", DOWN_PAIRS)
+def test_down_forward_and_backward(ops, cin, cout):
+    x, xr = _act((2, 6, 10, 36, cin), 6)
+    w = R.bf16(_rand((8, cin, cout), 7, 1.0 / np.sqrt(8 * cin)))
+    wt = R.down_weight(w)
+    stats = torch.empty((2, cout, 2), dtype=torch.float64, device="cuda")
+    y = ops.conv(1, x, ops.pack(w.float().cuda()), cout, stats=stats)
+    _close(y, R.ndhwc(F.conv3d(R.ncdhw(xr), wt, stride=2)))
+    dy, dyr = _act((2, 3, 5, 18, cout), 8)
+    # backward-data: transposed conv with transposed weights
+    dx = ops.conv_up(dy, ops.pack(w.float().cuda(), 0, 1), cin)
+    _close(dx, R.ndhwc(torch.nn.grad.conv3d_input(R.ncdhw(xr).shape, wt, R.ncdhw(dyr), stride=2)))
+    # accumulate into an existing gradient (the encoder skip)
+    acc, accr = _act((2, 6, 10, 36, cin), 9)
+    ops.conv_up(dy, ops.pack(w.float().cuda(), 0, 1), cin, addend=acc, out=acc)
+    _close(acc, accr + R.ndhwc(torch.nn.grad.conv3d_input(R.ncdhw(xr).shape, wt, R.ncdhw(dyr), stride=2)))
+    g = ops.wgrad(1, x, dy, cin)
+    ref_w = torch.nn.grad.conv3d_weight(R.ncdhw(xr), wt.shape, R.ncdhw(dyr), stride=2)
+    _close(g, ref_w.permute(2, 3, 4, 1, 0).reshape(8, cin, cout), rtol=1e-4, atol_frac=1e-4)
+
+
+@pytest.mark.parametrize("cin,cout", UP_PAIRS)
+def test_up_forward_and_backward(ops, cin, cout):
+    x, xr = _act((1, 3, 5, 9, cin), 10)
+    skip, skipr = _act((1, 6, 10, 18, cout), 11)
+    w = R.bf16(_rand((8, cout, cin), 12, 1.0 / np.sqrt(cin)))
+    wt = R.up_weight(w)
+    y = ops.conv_up(x, ops.pack(w.float().cuda(), 0, 1), cout, addend=skip)
+    _close(y, R.ndhwc(F.conv_transpose3d(R.ncdhw(xr), wt, stride=2)) + skipr)
+    dy, dyr = _act((1, 6, 10, 18, cout), 13)
+    # backward-data: 2x2x2 stride-2 gather over the fine gradient
+    dx = ops.conv(1, dy, ops.pack(w.float().cuda(), 0, 0), cin)
+    xt = R.ncdhw(xr).clone().requires_grad_(True)
+    F.conv_transpose3d(xt, wt, stride=2).backward(R.ncdhw(dyr))
+    _close(dx, R.ndhwc(xt.grad))
+    # backward-weight: P = fine gradient, Q = coarse input -> [8][cout][cin]
+    g = ops.wgrad(1, dy, x, cout)
+    wv = wt.clone().requires_grad_(True)
+    F.conv_transpose3d(R.ncdhw(xr), wv, stride=2).backward(R.ncdhw(dyr))
+    ref_g = wv.grad.permute(2, 3, 4, 1, 0).reshape(8, cout, cin)  # (cin,cout,dz,dy,dx) -> [t][cout][cin]
+    _close(g, ref_g, rtol=1e-4, atol_frac=1e-4)
+
+
+@pytest.mark.parametrize("c", [16, 32, 128])
+def test_norm_act_forward_backward(ops, c):
+    n, shape = 2, (4, 6, 10)
+    y, yr = _act((n,) + shape + (c,), 14)
+    yr = yr * 3.0 + 1.5
+    y = yr.to(torch.bfloat16).cuda()
+    yr = R.bf16(yr)
+    gamma = _rand((c,), 15, 0.3).abs() + 0.5
+    beta = _rand((c,), 16, 0.2)
+    slope, eps = 0.01, 1e-5
+    stats = torch.stack([yr.sum(dim=(1, 2, 3)), (yr * yr).sum(dim=(1, 2, 3))], dim=-1).cuda()
+    count = int(np.prod(shape))
+    coef = ops.norm_finalize(stats, count, gamma.float().cuda(), beta.float().cuda(), eps)
+    a = ops.norm_act(y, coef, slope)
+    yt = R.ncdhw(yr).clone().requires_grad_(True)
+    gt = gamma.clone().requires_grad_(True)
+    bt = beta.clone().requires_grad_(True)
+    ref = R.norm_act(yt, gt, bt, eps, slope)
+    _close(a, R.ndhwc(ref.detach()))
+    da, dar = _act((n,) + shape + (c,), 17)
+    ref.backward(R.ncdhw(dar))
+    dy, dg, db = ops.norm_act_bwd(y, da, coef, gamma.float().cuda(), slope)
+    _close(dy, R.ndhwc(yt.grad), rtol=2e-2, atol_frac=5e-3)
+    _close(dg, gt.grad, rtol=1e-3, atol_frac=1e-3)
+    _close(db, bt.grad, rtol=1e-3, atol_frac=1e-3)
+
+
+def test_head_and_loss(ops):
+    vox = 3000
+    g, gr = _act((1, vox, 1, 1, 16), 18)
+    w = _rand((16,), 19, 0.3)
+    b = torch.tensor([0.1], dtype=torch.float64)
+    target = _rand((vox,), 20).abs()
+    target[::7] = -1.0
+    tgt = target.float().cuda()
+    pred = ops.head(g, w.float().cuda(), b.float().cuda(), tgt, -0.5, 1.0)
+    g2 = gr.reshape(vox, 16)
+    ref_pred = torch.where(target >= 0, g2 @ w + b, torch.zeros(vox, dtype=torch.float64))
+    _close(pred, ref_pred, rtol=1e-5, atol_frac=1e-5)
+    inv = 1.0 / float((target >= 0).sum())
+    loss, dg, dw, db = ops.head_loss_bwd(g, w.float().cuda(), pred, tgt, inv)
+    gt = g2.clone().requires_grad_(True)
+    wt = w.clone().requires_grad_(True)
+    bt = b.clone().requires_grad_(True)
+    p = gt @ wt + bt
+    act = target >= 0
+    L = (torch.where(act, p - target, torch.zeros_like(p)) ** 2).sum() * inv
+    L.backward()
+    assert abs(float(loss.cpu()) - float(L)) <= 1e-5 * float(L)
+    _close(dg.reshape(vox, 16), gt.grad, rtol=1e-2, atol_frac=1e-2)
+    _close(dw, wt.grad, rtol=1e-4, atol_frac=1e-4)
+    _close(db, bt.grad, rtol=1e-4, atol_frac=1e-4)
+
+
+def _rel_l2(got, ref):
+    got = got.detach().double().cpu().reshape(-1)
+    ref = ref.double().reshape(-1)
+    return float((got - ref).norm() / ref.norm().clamp_min(1e-30))
+
+
+def _cos(a, b):
+    a = a.detach().double().cpu().reshape(-1)
+    b = b.double().reshape(-1)
+    return float(a @ b / (a.norm() * b.norm()).clamp_min(1e-300))
+
+
+@pytest.fixture(scope="module")
+def network_case():
+    from dosecuda_b200.surrogate import SurrogateNet
+    net = SurrogateNet(device="cuda", seed=3)
+    shape = (16, 24, 32)
+    gen = torch.Generator().manual_seed(21)
+    terma = torch.rand(shape, generator=gen) * 2.0
+    density = 0.2 + torch.rand(shape, generator=gen)
+    terma[:, :, :5] = 0.0
+    x8 = net.ops.pack_input(terma.cuda(), density.cuda(), net.terma_scale)
+    target = torch.where(terma > 0.01, torch.rand(shape, generator=gen), torch.full(shape, -1.0)).reshape(-1)
+    inv = 1.0 / float((target >= 0).sum())
+    trace = {}
+    cache = {}
+    g0 = net.features(x8, cache)
+    w, b = net.params["head.w"], net.params["head.b"]
+    pred = net.ops.head(g0, w, b, target.cuda(), -0.5, 1.0)
+    loss, dg0, dw, db = net.ops.head_loss_bwd(g0, w, pred, target.cuda(), inv)
+    grads = net.backward(cache, dg0, trace)
+    grads["head.w"], grads["head.b"] = dw, db
+    torch.cuda.synchronize()
+    return net, x8, target, inv, cache, trace, grads, dg0, loss, g0
+
+
+def test_network_backward_teacher_forced(network_case):
+    """Every backward op of the encoder-decoder, recomputed in float64 from the
+    GPU's own forward activations and upstream gradients, wired as the
+    network's chain rule says: parameter gradients and activation gradients
+    agree to the single-kernel tolerances, so each op is right in place and
+    receives the right tensors."""
+    net, x8, target, inv, cache, tr, grads, dg0, loss, g0 = network_case
+    d = lambda t: t.detach().double().cpu()
+    W = {k: R.bf16(v.detach().cpu().double()) for k, v in net.params.items() if k.endswith(".w")}
+
+    def norm_bwd(name, da):
+        x, y, coef = cache[name]
+        yt = R.ncdhw(d(y)).clone().requires_grad_(True)
+        gam = net.params[name + ".gamma"].detach().cpu().double().requires_grad_(True)
+        bet = net.params[name + ".beta"].detach().cpu().double().requires_grad_(True)
+        R.norm_act(yt, gam, bet, net.eps, net.slope).backward(R.ncdhw(d(da)))
+        return R.ndhwc(yt.grad), gam.grad, bet.grad
+
+    def conv3_dx(name, dy, like):
+        return R.ndhwc(torch.nn.grad.conv3d_input(R.ncdhw(d(like)).shape, R.conv3_weight(W[name + ".w"]),
+                                                  R.ncdhw(d(dy)), padding=1))
+
+    def down_dx(name, dy, like):
+        return R.ndhwc(torch.nn.grad.conv3d_input(R.ncdhw(d(like)).shape, R.down_weight(W[name + ".w"]),
+                                                  R.ncdhw(d(dy)), stride=2))
+
+    def up_dx(name, dy, like):
+        xt = R.ncdhw(d(like)).clone().requires_grad_(True)
+        F.conv_transpose3d(xt, R.up_weight(W[name + ".w"]), stride=2).backward(R.ncdhw(d(dy)))
+        return R.ndhwc(xt.grad)
+
+    def w_grad(name, kind, x, dy):
+        if kind == "conv3":
+            g = torch.nn.grad.conv3d_weight(R.ncdhw(d(x)), R.conv3_weight(W[name + ".w"]).shape, R.ncdhw(d(dy)),
+                                            padding=1)
+            return g.permute(2, 3, 4, 1, 0).reshape(27, g.shape[1], g.shape[0])
+        g = torch.nn.grad.conv3d_weight(R.ncdhw(d(x)), R.down_weight(W[name + ".w"]).shape, R.ncdhw(d(dy)),
+                                        stride=2)
+        return g.permute(2, 3, 4, 1, 0).reshape(8, g.shape[1], g.shape[0])
+
+    def up_w_grad(name, x, dy):
+        wv = R.up_weight(W[name + ".w"]).clone().requires_grad_(True)
+        F.conv_transpose3d(R.ncdhw(d(x)), wv, stride=2).backward(R.ncdhw(d(dy)))
+        return wv.grad.permute(2, 3, 4, 1, 0).reshape(8, wv.shape[1], wv.shape[0])
+
+    def check_block(name, kind, da):
+        ref_dy, ref_dg, ref_db = norm_bwd(name, da)
+        _close(tr["dy." + name], ref_dy, rtol=2e-2, atol_frac=5e-3)
+        _close(grads[name + ".gamma"], ref_dg, rtol=1e-3, atol_frac=1e-3)
+        _close(grads[name + ".beta"], ref_db, rtol=1e-3, atol_frac=1e-3)
+        x = cache[name][0]
+        _close(grads[name + ".w"], w_grad(name, kind, x, tr["dy." + name]), rtol=1e-3, atol_frac=1e-3)
+
+    # decoder
+    check_block("dec0", "conv3", dg0)
+    _close(tr["u0"], conv3_dx("dec0", tr["dy.dec0"], tr["u0"]))
+    _close(grads["up0.w"], up_w_grad("up0", cache["g1"], tr["u0"]), rtol=1e-3, atol_frac=1e-3)
+    _close(tr["g1"], up_dx("up0", tr["u0"], cache["g1"]))
+    check_block("dec1", "conv3", tr["g1"])
+    _close(tr["u1"], conv3_dx("dec1", tr["dy.dec1"], tr["u1"]))
+    _close(grads["up1.w"], up_w_grad("up1", cache["g2"], tr["u1"]), rtol=1e-3, atol_frac=1e-3)
+    _close(tr["g2"], up_dx("up1", tr["u1"], cache["g2"]))
+    check_block("dec2", "conv3", tr["g2"])
+    _close(tr["u2"], conv3_dx("dec2", tr["dy.dec2"], tr["u2"]))
+    _close(grads["up2.w"], up_w_grad("up2", cache["b"], tr["u2"]), rtol=1e-3, atol_frac=1e-3)
+    _close(tr["b"], up_dx("up2", tr["u2"], cache["b"]))
+    # encoder: d(e_k) = d(u_k) + down_k^T d(y_down_k)
+    check_block("bott", "conv3", tr["b"])
+    _close(tr["d2"], conv3_dx("bott", tr["dy.bott"], tr["d2"]))
+    check_block("down2", "down", tr["d2"])
+    _close(tr["e2"], d(tr["u2"]) + down_dx("down2", tr["dy.down2"], tr["e2"]))
+    check_block("enc2", "conv3", tr["e2"])
+    _close(tr["d1"], conv3_dx("enc2", tr["dy.enc2"], tr["d1"]))
+    check_block("down1", "down", tr["d1"])
+    _close(tr["e1"], d(tr["u1"]) + down_dx("down1", tr["dy.down1"], tr["e1"]))
+    check_block("enc1", "conv3", tr["e1"])
+    _close(tr["d0"], conv3_dx("enc1", tr["dy.enc1"], tr["d0"]))
+    check_block("down0", "down", tr["d0"])
+    _close(tr["e0"], d(tr["u0"]) + down_dx("down0", tr["dy.down0"], tr["e0"]))
+    check_block("enc0", "conv3", tr["e0"])
+
+
+def test_network_against_float64_reference(network_case):
+    """End to end against the float64 reference that rounds to bf16 wherever
+    the kernels store bf16.  A randomly initialised 13-layer network with
+    instance norms is sensitive: moving 0.1 % of the stored values by one bf16
+    ulp changes the reference's own features by ~1 % and its encoder
+    gradients by up to ~25 % (relative L2).  The bounds below sit at that
+    level; gradient directions agree closely (cosine), and the loss and the
+    output-side gradients agree tightly.  The per-op agreement is the
+    teacher-forced test above."""
+    net, x8, target, inv, cache, tr, grads, dg0, loss, g0 = network_case
+    params = {}
+    for k, v in net.params.items():
+        t = v.detach().cpu().double()
+        params[k] = (R.bf16(t) if k.endswith(".w") and not k.startswith("head") else t).requires_grad_(True)
+    x8r = x8.double().cpu()
+    L = R.loss(params, x8r, target.double(), inv, net.slope, net.eps, bf16_points=True)
+    L.backward()
+    with torch.no_grad():
+        f = R.ndhwc(R.forward(params, x8r, net.slope, net.eps, bf16_points=True))
+    assert _rel_l2(g0, f) < 2e-2
+    assert abs(float(loss.cpu()) - float(L.detach())) < 1e-3 * float(L.detach())
+    for k in ("head.w", "head.b", "dec0.gamma", "dec0.beta", "dec0.w"):
+        assert _rel_l2(grads[k], params[k].grad) < 3e-2, k
+    worst = {k: _rel_l2(grads[k], p.grad) for k, p in params.items()}
+    assert max(worst.values()) < 0.35, worst
+    cos = {k: _cos(grads[k], p.grad) for k, p in params.items()}
+    assert min(cos.values()) > 0.94, cos
+    ga = torch.cat([grads[k].detach().double().cpu().reshape(-1) / params[k].grad.norm() for k in params])
+    gb = torch.cat([params[k].grad.reshape(-1) / params[k].grad.norm() for k in params])
+    assert _cos(ga, gb) > 0.98
