@@ -157,7 +157,7 @@ SIGNATURES = {
                               C.c_float, C.c_float, C.c_void_p, C.c_void_p]),
     "dc_net_head_loss_bwd": (C.c_int, [C.c_int, C.c_void_p, C.c_longlong, C.c_int, C.c_void_p, C.c_void_p,
                                        C.c_void_p, C.c_float, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
-                                       C.c_void_p]),
+                                       C.c_void_p, C.c_void_p]),
 }
 
 _lib = None

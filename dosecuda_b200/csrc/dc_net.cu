@@ -16,7 +16,10 @@
 // padding), and then runs every tap from shared memory.
 #include <algorithm>
 #include <cstdio>
+#include <map>
+#include <mutex>
 #include <string>
+#include <utility>
 
 #include "../../include/dosecuda.h"
 #include "dc_net.cuh"
@@ -684,9 +687,11 @@ __global__ void head_fwd_kernel(const uint4 *__restrict__ g, long long vox, cons
 __global__ void __launch_bounds__(256) head_loss_bwd_kernel(const uint4 *__restrict__ g, long long vox,
                                                             const float *__restrict__ w,
                                                             const float *__restrict__ pred,
-                                                            const float *__restrict__ target, float inv_count,
+                                                            const float *__restrict__ target, float inv_count_arg,
+                                                            const float *__restrict__ inv_count_dev,
                                                             double *__restrict__ loss, uint4 *__restrict__ dg,
                                                             float *__restrict__ dw, float *__restrict__ dbias) {
+    const float inv_count = inv_count_dev ? *inv_count_dev : inv_count_arg;
     __shared__ float s_w[16];
     __shared__ float s_acc[18];
     if (threadIdx.x < 16) s_w[threadIdx.x] = w[threadIdx.x];
@@ -776,10 +781,20 @@ unsigned elementwise_blocks(long long work, int threads) {
     return (unsigned)std::max(1LL, std::min(want, cap));
 }
 
+// Dynamic shared-memory opt-in, once per kernel instantiation and device
+// (so that launches inside a CUDA-graph capture make no attribute calls).
 template <class K>
 void set_smem(K kernel, size_t bytes) {
-    // idempotent; cheap enough to repeat per launch (host-side attribute)
+    static std::mutex mu;
+    static std::map<std::pair<const void *, int>, size_t> done;  // (kernel, device) -> opted-in bytes
+    int dev = 0;
+    DC_CUDA(cudaGetDevice(&dev));
+    const auto key = std::make_pair(reinterpret_cast<const void *>(kernel), dev);
+    std::lock_guard<std::mutex> lk(mu);
+    auto it = done.find(key);
+    if (it != done.end() && it->second >= bytes) return;
     DC_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+    done[key] = bytes;
 }
 
 template <int MODE, int CC, int NT, int TY, int TZ>
@@ -1035,7 +1050,8 @@ void head_fwd(const bf16 *g, long long vox, int c, const float *w, const float *
 }
 
 void head_loss_bwd(const bf16 *g, long long vox, int c, const float *w, const float *pred, const float *target,
-                   float inv_count, double *loss, bf16 *dg, float *dw, float *dbias, cudaStream_t s) {
+                   float inv_count, const float *inv_count_dev, double *loss, bf16 *dg, float *dw, float *dbias,
+                   cudaStream_t s) {
     need(g && w && pred && target && loss && dg && dw && dbias, "head buffers must not be NULL");
     need(c == 16, "the output head takes 16 channels");
     need(vox > 0, "head volume must be positive");
@@ -1044,8 +1060,8 @@ void head_loss_bwd(const bf16 *g, long long vox, int c, const float *w, const fl
     DC_CUDA(cudaMemsetAsync(dw, 0, sizeof(float) * 16, s));
     DC_CUDA(cudaMemsetAsync(dbias, 0, sizeof(float), s));
     head_loss_bwd_kernel<<<elementwise_blocks(vox, 256), 256, 0, s>>>(
-        reinterpret_cast<const uint4 *>(g), vox, w, pred, target, inv_count, loss, reinterpret_cast<uint4 *>(dg), dw,
-        dbias);
+        reinterpret_cast<const uint4 *>(g), vox, w, pred, target, inv_count, inv_count_dev, loss,
+        reinterpret_cast<uint4 *>(dg), dw, dbias);
     check_launch("head_loss_bwd_kernel");
 }
 
@@ -1155,12 +1171,14 @@ int dc_net_head(int gpu_id, const void *g_dev, long long vox, int c, const float
 }
 
 int dc_net_head_loss_bwd(int gpu_id, const void *g_dev, long long vox, int c, const float *w_dev,
-                         const float *pred_dev, const float *target_dev, float inv_count, double *loss_dev,
-                         void *dg_dev, float *dw_dev, float *dbias_dev, void *stream) {
+                         const float *pred_dev, const float *target_dev, float inv_count,
+                         const float *inv_count_dev, double *loss_dev, void *dg_dev, float *dw_dev, float *dbias_dev,
+                         void *stream) {
     return guarded([&] {
         select_device(gpu_id);
-        net::head_loss_bwd(static_cast<const bf16 *>(g_dev), vox, c, w_dev, pred_dev, target_dev, inv_count, loss_dev,
-                           static_cast<bf16 *>(dg_dev), dw_dev, dbias_dev, as_stream(stream));
+        net::head_loss_bwd(static_cast<const bf16 *>(g_dev), vox, c, w_dev, pred_dev, target_dev, inv_count,
+                           inv_count_dev, loss_dev, static_cast<bf16 *>(dg_dev), dw_dev, dbias_dev,
+                           as_stream(stream));
     });
 }
 

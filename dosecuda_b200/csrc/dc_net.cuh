@@ -56,7 +56,8 @@ void pack_input(const float *terma, const float *density, long long vox, float t
 void head_fwd(const bf16 *g, long long vox, int c, const float *w, const float *bias, const float *mask,
               float mask_thr, float scale, float *out, cudaStream_t s);
 void head_loss_bwd(const bf16 *g, long long vox, int c, const float *w, const float *pred, const float *target,
-                   float inv_count, double *loss, bf16 *dg, float *dw, float *dbias, cudaStream_t s);
+                   float inv_count, const float *inv_count_dev, double *loss, bf16 *dg, float *dw, float *dbias,
+                   cudaStream_t s);
 
 }  // namespace net
 }  // namespace dc

@@ -90,13 +90,16 @@ class NetOps:
     def _act(self, shape):
         return torch.empty(shape, dtype=torch.bfloat16, device=self.device)
 
-    def pack(self, master, flip=0, trans=0):
+    def pack(self, master, flip=0, trans=0, out=None):
         T, A, B = master.shape
         k, n = (B, A) if trans else (A, B)
         frags = self.lib.dc_net_packed_fragments(T, k, n)
         if frags < 0:
             raise ValueError("invalid weight shape for packing")
-        out = torch.empty(frags, dtype=torch.int64, device=self.device)
+        if out is None:
+            out = torch.empty(frags, dtype=torch.int64, device=self.device)
+        elif out.numel() != frags:
+            raise ValueError("packed weight buffer has the wrong size")
         _lib.raise_for(self.lib.dc_net_pack_weights(self.gpu, _ptr(master), T, A, B, flip, trans, _ptr(out),
                                                     self._s()))
         return out
@@ -167,15 +170,19 @@ class NetOps:
         return out
 
     def head_loss_bwd(self, g, w, pred, target, inv_count):
+        """inv_count: a float, or a one-element float32 device tensor (read at
+        run time, so a captured graph can be replayed with new values)."""
         c = g.shape[-1]
         vox = g.numel() // c
         loss = torch.empty(1, dtype=torch.float64, device=self.device)
         dg = torch.empty_like(g)
         dw = torch.empty(c, dtype=torch.float32, device=self.device)
         db = torch.empty(1, dtype=torch.float32, device=self.device)
+        inv_dev = inv_count if isinstance(inv_count, torch.Tensor) else None
+        inv_val = 0.0 if inv_dev is not None else float(inv_count)
         _lib.raise_for(self.lib.dc_net_head_loss_bwd(self.gpu, _ptr(g), vox, c, _ptr(w), _ptr(pred), _ptr(target),
-                                                     float(inv_count), _ptr(loss), _ptr(dg), _ptr(dw), _ptr(db),
-                                                     self._s()))
+                                                     inv_val, _ptr(inv_dev), _ptr(loss), _ptr(dg), _ptr(dw),
+                                                     _ptr(db), self._s()))
         return loss, dg, dw, db
 
 
@@ -211,20 +218,17 @@ class SurrogateNet:
     # -- parameters ----------------------------------------------------------
     def repack(self):
         """bf16 fragment-order copies of the master weights: forward, and the
-        backward-data form (flipped/transposed) of each layer."""
+        backward-data form (flipped/transposed) of each layer.  The packed
+        buffers are allocated once and rewritten in place, so CUDA graphs
+        captured over the forward/backward see every update."""
         ops = self.ops
+        forms = {"conv3": ((0, 0), (1, 1)), "down": ((0, 0), (0, 1)), "up": ((0, 1), (0, 0))}
         for name, kind, _, _ in ARCH:
             w = self.params[name + ".w"]
-            if kind == "conv3":
-                self._fw[name] = ops.pack(w, 0, 0)
-                if name != "enc0":
-                    self._bw[name] = ops.pack(w, 1, 1)
-            elif kind == "down":
-                self._fw[name] = ops.pack(w, 0, 0)
-                self._bw[name] = ops.pack(w, 0, 1)
-            else:
-                self._fw[name] = ops.pack(w, 0, 1)
-                self._bw[name] = ops.pack(w, 0, 0)
+            (ff, ft), (bf, bt) = forms[kind]
+            self._fw[name] = ops.pack(w, ff, ft, out=self._fw.get(name))
+            if name != "enc0":
+                self._bw[name] = ops.pack(w, bf, bt, out=self._bw.get(name))
 
     def parameters(self):
         return list(self.params.values())
@@ -522,40 +526,93 @@ class Dataset:
         return len(self.seeds)
 
 
+class Trainer:
+    """One training step (input packing, forward, loss, backward, Adam,
+    weight repacking) on static device buffers, captured once in a CUDA graph
+    and replayed per sample; eager when capture is disabled."""
+
+    def __init__(self, net: SurrogateNet, shape, lr=1e-3, use_graph=True):
+        self.net = net
+        dev = net.device
+        self.shape = tuple(shape)
+        self.terma = torch.zeros(self.shape, dtype=torch.float32, device=dev)
+        self.density = torch.zeros(self.shape, dtype=torch.float32, device=dev)
+        self.target = torch.full((int(np.prod(self.shape)),), -1.0, dtype=torch.float32, device=dev)
+        self.inv = torch.ones(1, dtype=torch.float32, device=dev)
+        self.x8 = None
+        self.lr = torch.tensor(float(lr), dtype=torch.float32, device=dev)
+        for p in net.parameters():
+            p.grad = torch.zeros_like(p)
+        self.opt = torch.optim.Adam(net.parameters(), lr=self.lr, capturable=True)
+        self.loss_sum = torch.zeros((), dtype=torch.float64, device=dev)
+        self.use_graph = use_graph
+        self.graph = None
+        self.steps = 0
+
+    def _step(self):
+        net = self.net
+        self.x8 = net.ops.pack_input(self.terma, self.density, net.terma_scale, out=self.x8)
+        loss, grads = net.loss_and_grads(self.x8, self.target, self.inv)
+        for k, p in net.params.items():
+            p.grad.copy_(grads[k])
+        self.opt.step()
+        net.repack()
+        self.loss_sum += loss[0]
+
+    def load(self, terma, density, target, inv_count):
+        self.terma.copy_(terma)
+        self.density.copy_(density)
+        self.target.copy_(target.reshape(-1))
+        self.inv.fill_(float(inv_count))
+
+    def step(self):
+        """One step on the loaded sample."""
+        if self.use_graph and self.graph is None and self.steps >= 3:
+            # capture after three eager steps (Adam's state exists by then)
+            side = torch.cuda.Stream(self.net.device)
+            side.wait_stream(torch.cuda.current_stream(self.net.device))
+            g = torch.cuda.CUDAGraph()
+            with torch.cuda.stream(side):
+                with torch.cuda.graph(g, stream=side):
+                    self._step()
+            torch.cuda.current_stream(self.net.device).wait_stream(side)
+            self.graph = g
+        if self.graph is not None:
+            self.graph.replay()
+        else:
+            self._step()
+        self.steps += 1
+
+
 def train(net: SurrogateNet, data: Dataset, epochs=1, lr=1e-3, seed=0, log=None, max_steps=None,
-          time_budget_s=None, checkpoint=None):
-    """Adam (lr) on the squared error of the normalised dose, one sample per
+          time_budget_s=None, checkpoint=None, cosine=True, lr_min=1e-5, use_graph=True):
+    """Adam (lr, cosine-decayed to lr_min over the planned steps when
+    ``cosine``) on the squared error of the normalised dose, one sample per
     step, samples shuffled each epoch.  Returns a list of (step, epoch, mean
     loss of the last log interval, seconds)."""
-    opt = torch.optim.Adam(net.parameters(), lr=lr)
-    for p in net.parameters():
-        p.grad = torch.zeros_like(p)
+    tr = Trainer(net, data.maker.shape, lr=lr, use_graph=use_graph)
     rng = np.random.default_rng(seed)
-    dens32 = torch.empty(data.maker.shape, dtype=torch.float32, device=net.device)
-    x8 = None
+    total = epochs * len(data)
+    if max_steps:
+        total = min(total, max_steps)
     hist = []
-    step, t0 = 0, time.time()
-    acc, acc_n = torch.zeros((), dtype=torch.float64, device=net.device), 0
+    step, t0, last = 0, time.time(), 0
     stop = False
     for ep in range(epochs):
         for i in rng.permutation(len(data)):
-            dens32.copy_(data.density[i])
-            x8 = net.ops.pack_input(data.terma[i], dens32, net.terma_scale, out=x8)
-            loss, grads = net.loss_and_grads(x8, data.target[i].view(-1), float(data.inv_count[i]))
-            for k, p in net.params.items():
-                p.grad.copy_(grads[k])
-            opt.step()
-            net.repack()
-            acc += loss[0]
-            acc_n += 1
+            if cosine:
+                frac = min(step / max(total, 1), 1.0)
+                tr.lr.fill_(lr_min + 0.5 * (lr - lr_min) * (1.0 + math.cos(math.pi * frac)))
+            tr.load(data.terma[i], data.density[i], data.target[i], data.inv_count[i])
+            tr.step()
             step += 1
-            if log and step % 200 == 0:
-                m = float(acc) / acc_n
+            if log and step % 500 == 0:
+                m = float(tr.loss_sum) / (step - last)
+                tr.loss_sum.zero_()
+                last = step
                 hist.append((step, ep, m, time.time() - t0))
                 log("step %d epoch %d loss %.4e (%.1f s)" % (step, ep, m, time.time() - t0))
-                acc.zero_()
-                acc_n = 0
-            if (max_steps and step >= max_steps) or (time_budget_s and time.time() - t0 > time_budget_s):
+            if step >= total or (time_budget_s and time.time() - t0 > time_budget_s):
                 stop = True
                 break
         if checkpoint:
@@ -572,22 +629,53 @@ def train(net: SurrogateNet, data: Dataset, epochs=1, lr=1e-3, seed=0, log=None,
 class PhotonSurrogate:
     """Surrogate dose of one photon control point with CCCS fallback.
 
-    ``dose(density, cp)`` runs TERMA, the network, the CCCS probe and the
-    probe gamma; it returns (dose, accepted, pass_rate, n_probe_points).  A
-    rejected control point gets the full CCCS dose from the same TERMA."""
+    ``dose(density, cp)`` runs TERMA, the network (one CUDA-graph replay),
+    the CCCS probe and the probe gamma; it returns (dose, accepted,
+    pass_rate, n_probe_points).  A rejected control point gets the full CCCS
+    dose from the same TERMA."""
 
     def __init__(self, net: SurrogateNet, grid, shape, model, accept_rate=0.99, dta_mm=2.0, dd_frac=0.02,
-                 cutoff_frac=0.1):
+                 cutoff_frac=0.1, use_graph=True):
         from . import engine
         self.net, self.model = net, model
         self.grid, self.shape = grid, tuple(shape)
         self.accept_rate, self.dta, self.dd, self.cutoff = accept_rate, dta_mm, dd_frac, cutoff_frac
-        self.beam = engine.PhotonBeam(grid, shape, device=net.device)
-        self.terma = torch.empty(self.shape, dtype=torch.float32, device=net.device)
-        self.pred = torch.empty(self.shape, dtype=torch.float32, device=net.device)
-        self.counts = torch.empty(4, dtype=torch.int32, device=net.device)
+        dev = net.device
+        self.beam = engine.PhotonBeam(grid, shape, device=dev)
+        self.terma = torch.zeros(self.shape, dtype=torch.float32, device=dev)
+        self.density = torch.zeros(self.shape, dtype=torch.float32, device=dev)
+        self.pred = torch.zeros(self.shape, dtype=torch.float32, device=dev)
+        self.counts = torch.zeros(4, dtype=torch.int32, device=dev)
         self._x8 = None
         self._mv = None
+        self.use_graph = use_graph
+        self.graph = None
+        self._runs = 0
+
+    def _network(self):
+        """pred = network dose / dose_scale (masked where TERMA <= 0.01)."""
+        net = self.net
+        self._x8 = net.ops.pack_input(self.terma, self.density, net.terma_scale, out=self._x8)
+        g0 = net.features(self._x8)
+        net.ops.head(g0, net.params["head.w"], net.params["head.b"], self.terma, 0.01, net.dose_unit,
+                     out=self.pred.view(-1))
+
+    def run_network(self):
+        if self.use_graph and self.graph is None and self._runs >= 1:
+            dev = self.net.device
+            side = torch.cuda.Stream(dev)
+            side.wait_stream(torch.cuda.current_stream(dev))
+            g = torch.cuda.CUDAGraph()
+            with torch.cuda.stream(side):
+                with torch.cuda.graph(g, stream=side):
+                    self._network()
+            torch.cuda.current_stream(dev).wait_stream(side)
+            self.graph = g
+        if self.graph is not None:
+            self.graph.replay()
+        else:
+            self._network()
+        self._runs += 1
 
     def dose(self, density: torch.Tensor, cp, force_fallback=False):
         from . import engine
@@ -597,19 +685,18 @@ class PhotonSurrogate:
         views = (self._mv, ControlPointView(cp))
         scale = float(self.model.mu_calibration) * float(cp.mu)
         self.beam.set_density(density)
+        self.density.copy_(density)
         self.beam.terma(self.model, cp, out=self.terma, views=views)
-        self._x8 = self.net.ops.pack_input(self.terma, density, self.net.terma_scale, out=self._x8)
-        g0 = self.net.features(self._x8)
-        self.net.ops.head(g0, self.net.params["head.w"], self.net.params["head.b"], self.terma, 0.01,
-                          self.net.dose_unit * scale, out=self.pred.view(-1))
+        self.run_network()
         n = self.beam.select_probe()
         vp, n, _ = self.beam.probe_voxels()
         probe = self.beam.probe()
+        probe.mul_(1.0 / scale)  # to the network's units (gamma is scale-free)
         engine.gamma_counts(self.pred, self.grid.spacing, probe, vp, n, 0.0, self.dta, self.dd, self.cutoff,
                             counts=self.counts)
         ev, ps = (int(v) for v in self.counts[:2].cpu())
         rate = ps / ev if ev else 0.0
         accepted = (ev > 0 and rate >= self.accept_rate) and not force_fallback
         if accepted:
-            return self.pred, True, rate, n
+            return self.pred.mul_(scale), True, rate, n
         return self.beam.dose(), False, rate, n

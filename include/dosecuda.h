@@ -396,11 +396,14 @@ int dc_net_pack_input(int gpu_id, const float *terma_dev, const float *density_d
  * scale*(w.g + bias) : 0. */
 int dc_net_head(int gpu_id, const void *g_dev, long long vox, int c, const float *w_dev, const float *bias_dev,
                 const float *mask_dev, float mask_thr, float scale, float *out_dev, void *stream);
-/* Squared-error loss over voxels with target >= 0, times inv_count, and
- * its gradients: dg (16 channels), dw, dbias, loss (all overwritten). */
+/* Squared-error loss over voxels with target >= 0, times inv_count (read
+ * from inv_count_dev instead when that is not NULL, e.g. inside a CUDA
+ * graph), and its gradients: dg (16 channels), dw, dbias, loss (all
+ * overwritten). */
 int dc_net_head_loss_bwd(int gpu_id, const void *g_dev, long long vox, int c, const float *w_dev,
-                         const float *pred_dev, const float *target_dev, float inv_count, double *loss_dev,
-                         void *dg_dev, float *dw_dev, float *dbias_dev, void *stream);
+                         const float *pred_dev, const float *target_dev, float inv_count,
+                         const float *inv_count_dev, double *loss_dev, void *dg_dev, float *dw_dev,
+                         float *dbias_dev, void *stream);
 
 #ifdef __cplusplus
 }
