@@ -528,6 +528,101 @@ def run_optimisation(args, local, dist_mod):
     }
 
 
+SURROGATE_WEIGHTS = os.path.join(ROOT, "dosecuda_b200", "weights", "surrogate_6mv.npz")
+
+
+def run_surrogate(args, local, dist_mod):
+    """Learned photon surrogate with CCCS fallback on held-out phantoms of the
+    surrogate workload (128^3 @ 2.5 mm, random ellipsoids, random gantry and
+    MLC field): per beam the surrogate path (TERMA, network, sparse CCCS
+    probe, probe gamma, full CCCS when rejected) against the CCCS path (TERMA
+    + full CCCS), both timed with CUDA events; every network dose judged
+    against the full CCCS with gamma(2%/2mm)."""
+    import torch
+    from dosecuda_b200 import engine
+    from dosecuda_b200.surrogate import PhotonSurrogate, SampleMaker, SurrogateNet, hu_to_density, random_field, \
+        random_phantom_hu
+    if not os.path.exists(SURROGATE_WEIGHTS):
+        return {"unavailable": "no trained weights at dosecuda_b200/weights/surrogate_6mv.npz"}
+    dev = torch.device("cuda", local)
+    net = SurrogateNet.load(SURROGATE_WEIGHTS, device=dev)
+    maker = SampleMaker(device=dev)
+    sur = PhotonSurrogate(net, maker.grid, maker.shape, maker.model, accept_rate=0.99)
+    seeds = [1_000_000 + i for i in range(args.surrogate_beams)]
+    cases = []
+    for s in seeds:
+        rng = np.random.default_rng(s)
+        hu = random_phantom_hu(rng, maker.shape, maker.spacing, dev)
+        cases.append((hu_to_density(hu, *maker.table).contiguous(), maker.control_point(*random_field(rng))))
+    for _ in range(max(args.warmup, 3)):
+        sur.dose(*cases[0])
+        maker.beam.set_density(cases[0][0])
+        maker.beam.terma(maker.model, cases[0][1], views=maker.views(cases[0][1]))
+        maker.beam.dose()
+    torch.cuda.synchronize()
+    barrier(dist_mod)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    judge = torch.empty(4, dtype=torch.int32, device=dev)
+    rows = []
+    for density, cp in cases:
+        ev[0].record()
+        dose, accepted, rate, n_probe = sur.dose(density, cp)
+        ev[1].record()
+        torch.cuda.synchronize()
+        net_dose = sur.pred.clone() if accepted else sur.pred * maker.dose_scale(cp)
+        ev[2].record()
+        maker.beam.set_density(density)
+        maker.beam.terma(maker.model, cp, views=maker.views(cp))
+        cccs = maker.beam.dose()
+        ev[3].record()
+        torch.cuda.synchronize()
+        dmax = float(cccs.max())
+        engine.gamma_counts(net_dose, maker.grid.spacing, cccs, dose_norm=dmax, counts=judge)
+        e, p = (int(v) for v in judge[:2].cpu())
+        rows.append((ev[0].elapsed_time(ev[1]), ev[2].elapsed_time(ev[3]), bool(accepted), rate, p / max(e, 1),
+                     n_probe))
+    t_sur = aggregate_max(float(np.mean([r[0] for r in rows])), dist_mod)
+    t_cccs = aggregate_max(float(np.mean([r[1] for r in rows])), dist_mod)
+    acc = [r for r in rows if r[2]]
+    # network forward alone (one CUDA-graph replay), and the conv-stack roofline
+    k = max(args.steps, 5)
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(k):
+        sur.run_network()
+    b.record()
+    torch.cuda.synchronize()
+    t_net = a.elapsed_time(b) / k
+    flops = SurrogateNet.flops(maker.shape)
+    pk, pk_kind = peaks()
+    bf16_peak = pk.get("bf16_tflops", PEAKS_FALLBACK["bf16_tflops"])
+    achieved = flops / (t_net * 1e-3) / 1e12
+    return {
+        "metric": "surrogate vs CCCS speed-up at gamma(2%/2mm) >= 99% (per beam, fallbacks included)",
+        "value": round(t_cccs / t_sur, 3), "unit": "x", "higher_is_better": True,
+        "ms_per_beam_surrogate_path": round(t_sur, 4), "ms_per_beam_cccs_path": round(t_cccs, 4),
+        "ms_per_beam_accepted": round(float(np.mean([r[0] for r in acc])), 4) if acc else None,
+        "beams": len(rows), "accepted_frac": round(len(acc) / len(rows), 4),
+        "judge_pass_mean_accepted": round(float(np.mean([r[4] for r in acc])), 5) if acc else None,
+        "judge_pass_min_accepted": round(float(np.min([r[4] for r in acc])), 5) if acc else None,
+        "false_accepts": int(sum(1 for r in acc if r[4] < 0.99)),
+        "judge_pass_mean_all": round(float(np.mean([r[4] for r in rows])), 5),
+        "probe_points_mean": round(float(np.mean([r[5] for r in rows])), 1),
+        "network_forward_ms": round(t_net, 4),
+        "roofline": {"bound": "tensor", "kernel": "conv stack (bf16 mma.sync implicit GEMM)",
+                     "achieved": round(achieved, 2), "peak": bf16_peak, "unit": "TFLOP/s",
+                     "frac": round(achieved / bf16_peak, 4), "peak_kind": pk_kind,
+                     "work": "%d FLOPs per forward (conv layers counted from their shapes + head)" % flops},
+        "config": {"workload": "photon surrogate: 128^3 @ 2.5 mm, water body + 1-5 random ellipsoids (HU -900..1500), "
+                               "6 MV, gantry 0-355 in 5 deg steps, 2-20 cm MLC fields, 100 MU; held-out seeds "
+                               "1000000+i",
+                   "network": "4-level 3D encoder-decoder, 16-128 channels, bf16 activations, fp32 accumulation",
+                   "acceptance": "probe gamma(2%/2mm, 10% cutoff) >= 99% on CCCS at ~%d probe voxels"
+                                 % int(np.mean([r[5] for r in rows])),
+                   "l2": "per-beam working set (activations) above the 126 MB L2"},
+    }
+
+
 def cpu_baseline_photon():
     """The FP64 C oracle on the host cores: one full control point of the
     photon workload (the whole 128^3 beam; about 10-30 s of CPU time).
@@ -565,6 +660,7 @@ def main_mine(args):
     r = run_mine(args, ws, rank, local, dist_mod)
     batched = run_batched(args, local, dist_mod, ws) if args.batch_plans > 0 else None
     optimisation = run_optimisation(args, local, dist_mod) if args.opt_iters > 0 else None
+    surrogate = run_surrogate(args, local, dist_mod) if args.surrogate_beams > 0 else None
     if rank == 0:
         cpu_x = cpu_p = None
         if ws == 1 and not args.no_cpu:
@@ -645,6 +741,7 @@ def main_mine(args):
             },
             "batched": batched,
             "optimisation": optimisation,
+            "surrogate": surrogate,
         }
         print(json.dumps(line))
     if dist_mod is not None:
@@ -771,6 +868,7 @@ def main():
     ap.add_argument("--batch-plans", type=int, default=16, help="plans in the batched workload (0: skip)")
     ap.add_argument("--opt-iters", type=int, default=200, help="optimisation iterations (0: skip)")
     ap.add_argument("--tune-cache", action="store_true", help="keep the tile autotuner's JSON cache")
+    ap.add_argument("--surrogate-beams", type=int, default=30, help="held-out beams for the surrogate (0: skip)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -129,6 +129,7 @@ SIGNATURES = {
     "dc_photon_beam_terma": (C.c_int, [C.c_void_p, C.POINTER(PhotonModel), C.POINTER(ControlPoint), C.c_void_p,
                                        C.c_void_p]),
     "dc_photon_beam_dose": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "dc_photon_beam_probe_config": (C.c_int, [C.c_void_p, C.c_int]),
     "dc_photon_beam_probe_select": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.c_void_p]),
     "dc_photon_beam_probe_list": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_int), C.c_void_p,
                                             C.c_int]),
@@ -148,6 +149,9 @@ SIGNATURES = {
                                        C.c_float, C.c_void_p, C.c_void_p]),
     "dc_net_norm_act": (C.c_int, [C.c_int, C.c_void_p, C.c_int, C.c_longlong, C.c_int, C.c_void_p, C.c_float,
                                   C.c_void_p, C.c_void_p]),
+    "dc_net_norm_stats_act": (C.c_int, [C.c_int, C.c_void_p, C.c_int, C.c_longlong, C.c_int, C.c_void_p,
+                                        C.c_longlong, C.c_void_p, C.c_void_p, C.c_float, C.c_float, C.c_void_p,
+                                        C.c_void_p, C.c_void_p]),
     "dc_net_norm_act_bwd": (C.c_int, [C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_longlong, C.c_int, C.c_void_p,
                                       C.c_void_p, C.c_float, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                       C.c_void_p]),

@@ -42,6 +42,11 @@ __device__ __forceinline__ void cp_async16(unsigned dst, const void *src, bool v
 }
 
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait_group() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
 
 __device__ __forceinline__ void ldsm_x4(unsigned addr, unsigned (&r)[4]) {
     asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];\n"
@@ -124,6 +129,31 @@ __device__ __forceinline__ void load_tile(uint4 *s, const bf16 *src, int ctot, i
     }
 }
 
+// Stage the packed weight fragments of k16 steps [s0, s0+G) (of S) and
+// n-tiles [j0, j0+NT) (of NTT) into dst, laid out [G][NT][32 lanes] uint2,
+// with cp.async (256 contiguous bytes per (step, n-tile)).
+template <int G, int NT>
+__device__ __forceinline__ void stage_weights(uint2 *dst, const uint2 *wt, int s0, int S, int NTT, int j0) {
+    constexpr int UNITS = G * NT * 16;
+    for (int u = threadIdx.x; u < UNITS; u += kThreads) {
+        const int q = u >> 4, part = u & 15;
+        const int g = q / NT, j = q % NT;
+        const int st = s0 + g;
+        if (st < S)
+            cp_async16(smem_u32(dst + (g * NT + j) * 32 + part * 2), wt + ((size_t)st * NTT + j0 + j) * 32 + part * 2,
+                       true);
+    }
+}
+
+// k16 steps staged per pipeline stage.
+template <int S, int NT>
+struct WeightStages {
+    static constexpr int G0 = NT >= 8 ? 4 : 8;
+    static constexpr int G = S < G0 ? S : G0;
+    static constexpr int CHUNKS = (S + G - 1) / G;
+    static constexpr int WORDS = G * NT * 32;  // uint2 per stage
+};
+
 // ---------------------------------------------------------------------------
 // Gather convolution (3x3x3 s1 p1, or 2x2x2 s2): forward, and the
 // backward-data pass of the 3x3x3 and of the transposed 2x2x2 convolution.
@@ -136,6 +166,7 @@ struct GatherArgs {
     int id, ih, iw;
     int od, oh, ow;
     int tiles_x, tiles_y, tiles_z;
+    int cout;  // total output channels; blockIdx.y selects a group of NT*8 of them
 };
 
 template <int MODE, int CC, int NT, int TY, int TZ>
@@ -144,10 +175,12 @@ __global__ void __launch_bounds__(kThreads) conv_gather_kernel(GatherArgs a) {
     constexpr int WM = TY * TZ / 4;  // output rows (m16 tiles) per warp
     constexpr int KCH = H::T * CC;   // 8-channel chunks along K
     constexpr int S = (KCH + 1) / 2; // k16 steps
-    constexpr int COUT = NT * 8;
+    constexpr int CG = NT * 8;  // output channels of this CTA
     static_assert(TY * TZ % 4 == 0, "4 warps share the rows of a tile");
     extern __shared__ uint4 smem[];
-    __shared__ float s_stat[2 * COUT];
+    __shared__ float s_stat[2 * CG];
+    const int NTT = a.cout / 8;          // n-tiles of the whole layer
+    const int j0 = blockIdx.y * NT;      // first n-tile of this CTA
 
     int b = blockIdx.x;
     const int tx = b % a.tiles_x;
@@ -159,6 +192,8 @@ __global__ void __launch_bounds__(kThreads) conv_gather_kernel(GatherArgs a) {
     const int ox0 = tx * 16, oy0 = ty * TY, oz0 = tz * TZ;
     const int tid = threadIdx.x;
 
+    using WS = WeightStages<S, NT>;
+    uint2 *sw = reinterpret_cast<uint2 *>(smem + H::N * CC);  // two weight stages after the tile
     {
         const bf16 *xs = a.x + (size_t)nb * a.id * a.ih * a.iw * (CC * 8);
         if (MODE == kConv3)
@@ -167,11 +202,11 @@ __global__ void __launch_bounds__(kThreads) conv_gather_kernel(GatherArgs a) {
         else
             load_tile<CC, MODE, H::HX, H::HY, H::HZ>(smem, xs, CC * 8, 0, a.id, a.ih, a.iw, 2 * oz0, 2 * oy0,
                                                      2 * ox0, a.x);
+        stage_weights<WS::G, NT>(sw, a.wt, 0, S, NTT, j0);
+        cp_async_commit();
     }
     if (a.stats)
-        for (int q = tid; q < 2 * COUT; q += kThreads) s_stat[q] = 0.f;
-    cp_async_wait_all();
-    __syncthreads();
+        for (int q = tid; q < 2 * CG; q += kThreads) s_stat[q] = 0.f;
 
     const int warp = tid >> 5, lane = tid & 31;
     const int lrow = (lane & 7) + ((lane >> 3) & 1) * 8;  // ldmatrix row = output x in the tile
@@ -188,24 +223,39 @@ __global__ void __launch_bounds__(kThreads) conv_gather_kernel(GatherArgs a) {
 #pragma unroll
             for (int e = 0; e < 4; ++e) acc[i][j][e] = 0.f;
 
-    const uint2 *wp = a.wt + lane;
     const unsigned sbase = smem_u32(smem);
+    // Weight pipeline: stage c+1 loads (cp.async) while stage c computes.
 #pragma unroll 1
-    for (int s = 0; s < S; ++s) {
-        uint2 bfr[NT];
-#pragma unroll
-        for (int j = 0; j < NT; ++j) bfr[j] = __ldg(wp + (s * NT + j) * 32);
-        int kc = 2 * s + khalf;
-        if ((KCH & 1) && kc >= KCH) kc = 0;  // padding chunk: its packed weights are zero
-        const int t = kc / CC, cc = kc % CC;
-        const int toff = tap_offset<MODE, H::HX, H::HY>(t);
-#pragma unroll
-        for (int i = 0; i < WM; ++i) {
-            unsigned af[4];
-            ldsm_x4(sbase + chunk_slot<CC, MODE>(hv0[i] + toff, cc) * 16, af);
-#pragma unroll
-            for (int j = 0; j < NT; ++j) mma_bf16(acc[i][j], af, bfr[j].x, bfr[j].y);
+    for (int c = 0; c < WS::CHUNKS; ++c) {
+        if (c + 1 < WS::CHUNKS) {
+            stage_weights<WS::G, NT>(sw + ((c + 1) & 1) * WS::WORDS, a.wt, (c + 1) * WS::G, S, NTT, j0);
+            cp_async_commit();
+            cp_async_wait_group<1>();
+        } else {
+            cp_async_wait_group<0>();
         }
+        __syncthreads();
+        const uint2 *wb = sw + (c & 1) * WS::WORDS + lane;
+#pragma unroll 1
+        for (int g = 0; g < WS::G; ++g) {
+            const int s = c * WS::G + g;
+            if (s >= S) break;
+            uint2 bfr[NT];
+#pragma unroll
+            for (int j = 0; j < NT; ++j) bfr[j] = wb[(g * NT + j) * 32];
+            int kc = 2 * s + khalf;
+            if ((KCH & 1) && kc >= KCH) kc = 0;  // padding chunk: its packed weights are zero
+            const int t = kc / CC, cc = kc % CC;
+            const int toff = tap_offset<MODE, H::HX, H::HY>(t);
+#pragma unroll
+            for (int i = 0; i < WM; ++i) {
+                unsigned af[4];
+                ldsm_x4(sbase + chunk_slot<CC, MODE>(hv0[i] + toff, cc) * 16, af);
+#pragma unroll
+                for (int j = 0; j < NT; ++j) mma_bf16(acc[i][j], af, bfr[j].x, bfr[j].y);
+            }
+        }
+        __syncthreads();  // stage (c & 1) is refilled by the next iteration
     }
 
     // Epilogue: bf16 store (+ instance-norm statistics of the stored values).
@@ -221,7 +271,7 @@ __global__ void __launch_bounds__(kThreads) conv_gather_kernel(GatherArgs a) {
         for (int hh = 0; hh < 2; ++hh) {
             const int ox = ox0 + crow + 8 * hh;
             if (ox >= a.ow || oy >= a.oh || oz >= a.od) continue;
-            bf16 *dst = a.y + ((((size_t)nb * a.od + oz) * a.oh + oy) * a.ow + ox) * COUT + ccol;
+            bf16 *dst = a.y + ((((size_t)nb * a.od + oz) * a.oh + oy) * a.ow + ox) * a.cout + 8 * j0 + ccol;
 #pragma unroll
             for (int j = 0; j < NT; ++j) {
                 const __nv_bfloat162 v = __floats2bfloat162_rn(acc[i][j][2 * hh], acc[i][j][2 * hh + 1]);
@@ -247,13 +297,14 @@ __global__ void __launch_bounds__(kThreads) conv_gather_kernel(GatherArgs a) {
                 }
                 if (lane < 4) {
                     atomicAdd(&s_stat[8 * j + ccol + e], u);
-                    atomicAdd(&s_stat[COUT + 8 * j + ccol + e], v);
+                    atomicAdd(&s_stat[CG + 8 * j + ccol + e], v);
                 }
             }
         __syncthreads();
-        for (int q = tid; q < COUT; q += kThreads) {
-            atomicAdd(&a.stats[((size_t)nb * COUT + q) * 2 + 0], (double)s_stat[q]);
-            atomicAdd(&a.stats[((size_t)nb * COUT + q) * 2 + 1], (double)s_stat[COUT + q]);
+        for (int q = tid; q < CG; q += kThreads) {
+            const size_t c = (size_t)nb * a.cout + 8 * j0 + q;
+            atomicAdd(&a.stats[c * 2 + 0], (double)s_stat[q]);
+            atomicAdd(&a.stats[c * 2 + 1], (double)s_stat[CG + q]);
         }
     }
 }
@@ -288,10 +339,12 @@ __global__ void __launch_bounds__(kThreads) conv_up_kernel(UpArgs a) {
     const int nb = b / a.tiles_z;
     const int ox0 = tx * 16, oy0 = ty * TY, oz0 = tz * TZ;
     const int tid = threadIdx.x;
+    constexpr int WORDS = S * NT * 32;  // one tap's weights per stage
+    uint2 *sw = reinterpret_cast<uint2 *>(smem + TZ * TY * 16 * CC);
     load_tile<CC, kConv3, 16, TY, TZ>(smem, a.x + (size_t)nb * a.d * a.h * a.w * (CC * 8), CC * 8, 0, a.d, a.h,
                                       a.w, oz0, oy0, ox0, a.x);
-    cp_async_wait_all();
-    __syncthreads();
+    stage_weights<S, NT>(sw, a.wt, 0, 8 * S, NT, 0);
+    cp_async_commit();
 
     const int warp = tid >> 5, lane = tid & 31;
     const int lrow = (lane & 7) + ((lane >> 3) & 1) * 8;
@@ -302,6 +355,15 @@ __global__ void __launch_bounds__(kThreads) conv_up_kernel(UpArgs a) {
 
 #pragma unroll 1
     for (int t = 0; t < 8; ++t) {
+        if (t + 1 < 8) {
+            stage_weights<S, NT>(sw + ((t + 1) & 1) * WORDS, a.wt, (t + 1) * S, 8 * S, NT, 0);
+            cp_async_commit();
+            cp_async_wait_group<1>();
+        } else {
+            cp_async_wait_group<0>();
+        }
+        __syncthreads();
+        const uint2 *wb = sw + (t & 1) * WORDS + lane;
         float acc[WM][NT][4];
 #pragma unroll
         for (int i = 0; i < WM; ++i)
@@ -313,7 +375,7 @@ __global__ void __launch_bounds__(kThreads) conv_up_kernel(UpArgs a) {
         for (int s = 0; s < S; ++s) {
             uint2 bfr[NT];
 #pragma unroll
-            for (int j = 0; j < NT; ++j) bfr[j] = __ldg(a.wt + ((t * S + s) * NT + j) * 32 + lane);
+            for (int j = 0; j < NT; ++j) bfr[j] = wb[(s * NT + j) * 32];
             const int cc = 2 * s + khalf;
 #pragma unroll
             for (int i = 0; i < WM; ++i) {
@@ -346,6 +408,7 @@ __global__ void __launch_bounds__(kThreads) conv_up_kernel(UpArgs a) {
                 }
             }
         }
+        __syncthreads();  // stage (t & 1) is refilled by the next iteration
     }
 }
 
@@ -531,6 +594,48 @@ __device__ __forceinline__ uint4 pack8(const float (&f)[8]) {
 #pragma unroll
     for (int i = 0; i < 4; ++i) h[i] = __floats2bfloat162_rn(f[2 * i], f[2 * i + 1]);
     return u;
+}
+
+// Instance-norm coefficients of (sample, channel) q from the convolution's
+// statistics (see norm_finalize_kernel).
+__device__ __forceinline__ float4 norm_coef(const double *stats, int q, int ch, double count, const float *gamma,
+                                           const float *beta, float eps) {
+    const double mean = stats[2 * q] / count;
+    const double var = fmax(stats[2 * q + 1] / count - mean * mean, 0.0);
+    const float rstd = (float)(1.0 / sqrt(var + (double)eps));
+    const float alpha = gamma[ch] * rstd;
+    return make_float4(alpha, beta[ch] - (float)mean * alpha, (float)mean, rstd);
+}
+
+// Finalize + apply in one pass: every block derives the coefficients of all
+// (sample, channel) pairs into shared memory (block 0 also stores them for
+// the backward pass), then a = lrelu(alpha*y + shift), 8 channels per thread.
+__global__ void norm_stats_act_kernel(const uint4 *__restrict__ y, long long chunks, int cc_per_vox, long long vox,
+                                      int n, int c, const double *__restrict__ stats, double count,
+                                      const float *__restrict__ gamma, const float *__restrict__ beta, float eps,
+                                      float slope, float4 *__restrict__ coef_out, uint4 *__restrict__ out) {
+    extern __shared__ float4 s_coef[];
+    for (int q = threadIdx.x; q < n * c; q += blockDim.x) {
+        const float4 k = norm_coef(stats, q, q % c, count, gamma, beta, eps);
+        s_coef[q] = k;
+        if (blockIdx.x == 0 && coef_out) coef_out[q] = k;
+    }
+    __syncthreads();
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < chunks;
+         q += (long long)gridDim.x * blockDim.x) {
+        const long long v = q / cc_per_vox;
+        const int cc = (int)(q - v * cc_per_vox);
+        const int nb = (int)(v / vox);
+        float f[8];
+        unpack8(__ldg(y + q), f);
+#pragma unroll
+        for (int e = 0; e < 8; ++e) {
+            const float4 k = s_coef[nb * c + cc * 8 + e];
+            const float z = fmaf(f[e], k.x, k.y);
+            f[e] = z > 0.f ? z : slope * z;
+        }
+        out[q] = pack8(f);
+    }
 }
 
 // a = lrelu(alpha*y + shift), 8 channels per thread.
@@ -804,12 +909,13 @@ void launch_gather(const GatherArgs &a0, int n, cudaStream_t s) {
     a.tiles_x = (a.ow + 15) / 16;
     a.tiles_y = (a.oh + TY - 1) / TY;
     a.tiles_z = (a.od + TZ - 1) / TZ;
-    const size_t smem = (size_t)H::N * CC * 16;
+    constexpr int S = (H::T * CC + 1) / 2;
+    const size_t smem = (size_t)H::N * CC * 16 + 2 * (size_t)WeightStages<S, NT>::WORDS * sizeof(uint2);
     auto k = conv_gather_kernel<MODE, CC, NT, TY, TZ>;
     set_smem(k, smem);
     const long long blocks = (long long)n * a.tiles_x * a.tiles_y * a.tiles_z;
     need(blocks < 0x7fffffffLL, "volume too large for the surrogate convolution");
-    k<<<(unsigned)blocks, kThreads, smem, s>>>(a);
+    k<<<dim3((unsigned)blocks, (unsigned)(a.cout / (8 * NT))), kThreads, smem, s>>>(a);
     check_launch("conv_gather_kernel");
 }
 
@@ -819,7 +925,7 @@ void launch_up(const UpArgs &a0, int n, cudaStream_t s) {
     a.tiles_x = (a.w + 15) / 16;
     a.tiles_y = (a.h + TY - 1) / TY;
     a.tiles_z = (a.d + TZ - 1) / TZ;
-    const size_t smem = (size_t)TZ * TY * 16 * CC * 16;
+    const size_t smem = (size_t)TZ * TY * 16 * CC * 16 + 2 * (size_t)(CC / 2) * NT * 32 * sizeof(uint2);
     auto k = conv_up_kernel<CC, NT, TY, TZ>;
     set_smem(k, smem);
     const long long blocks = (long long)n * a.tiles_x * a.tiles_y * a.tiles_z;
@@ -887,6 +993,7 @@ void conv_gather(int mode, const bf16 *x, int n, int d, int h, int w, int cin, c
     a.id = d;
     a.ih = h;
     a.iw = w;
+    a.cout = cout;
     if (mode == kConv3) {
         a.od = d;
         a.oh = h;
@@ -908,11 +1015,11 @@ void conv_gather(int mode, const bf16 *x, int n, int d, int h, int w, int cin, c
         if (cin == 16 && cout == 16) return launch_gather<kConv3, 2, 2, 8, 2>(a, n, s);
         if (cin == 32 && cout == 32) return launch_gather<kConv3, 4, 4, 8, 2>(a, n, s);
         if (cin == 64 && cout == 64) return launch_gather<kConv3, 8, 8, 8, 2>(a, n, s);
-        if (cin == 128 && cout == 128) return launch_gather<kConv3, 16, 16, 4, 2>(a, n, s);
+        if (cin == 128 && cout == 128) return launch_gather<kConv3, 16, 4, 4, 2>(a, n, s);  // 4 channel groups
     } else {
         if (cin == 16 && cout == 32) return launch_gather<kDown2, 2, 4, 8, 2>(a, n, s);
         if (cin == 32 && cout == 64) return launch_gather<kDown2, 4, 8, 4, 2>(a, n, s);
-        if (cin == 64 && cout == 128) return launch_gather<kDown2, 8, 16, 4, 2>(a, n, s);
+        if (cin == 64 && cout == 128) return launch_gather<kDown2, 8, 4, 4, 2>(a, n, s);  // 4 channel groups
     }
     throw Error(DC_ERR_VALUE, "unsupported convolution channels " + std::to_string(cin) + " -> " +
                                   std::to_string(cout));
@@ -1003,6 +1110,20 @@ void norm_act(const bf16 *y, int n, long long vox, int c, const float *coef, flo
         reinterpret_cast<const uint4 *>(y), chunks, c / 8, vox, c, reinterpret_cast<const float4 *>(coef), slope,
         reinterpret_cast<uint4 *>(out));
     check_launch("norm_act_kernel");
+}
+
+void norm_stats_act(const bf16 *y, int n, long long vox, int c, const double *stats, long long count,
+                    const float *gamma, const float *beta, float eps, float slope, float *coef, bf16 *out,
+                    cudaStream_t s) {
+    need(y && stats && gamma && beta && out, "norm buffers must not be NULL");
+    need(c % 8 == 0 && c <= 128, "norm channels must be a multiple of 8, at most 128");
+    need(n > 0 && n <= 16 && vox > 0 && count > 0, "norm volume must be positive (at most 16 samples)");
+    bind_device();
+    const long long chunks = (long long)n * vox * (c / 8);
+    norm_stats_act_kernel<<<elementwise_blocks(chunks, 256), 256, (size_t)n * c * sizeof(float4), s>>>(
+        reinterpret_cast<const uint4 *>(y), chunks, c / 8, vox, n, c, stats, (double)count, gamma, beta, eps, slope,
+        reinterpret_cast<float4 *>(coef), reinterpret_cast<uint4 *>(out));
+    check_launch("norm_stats_act_kernel");
 }
 
 void norm_act_bwd(const bf16 *y, const bf16 *da, int n, long long vox, int c, const float *coef, const float *gamma,
@@ -1139,6 +1260,16 @@ int dc_net_norm_act(int gpu_id, const void *y_dev, int n, long long vox, int c, 
         select_device(gpu_id);
         net::norm_act(static_cast<const bf16 *>(y_dev), n, vox, c, coef_dev, slope, static_cast<bf16 *>(a_dev),
                       as_stream(stream));
+    });
+}
+
+int dc_net_norm_stats_act(int gpu_id, const void *y_dev, int n, long long vox, int c, const double *stats_dev,
+                          long long count, const float *gamma_dev, const float *beta_dev, float eps, float slope,
+                          float *coef_dev, void *a_dev, void *stream) {
+    return guarded([&] {
+        select_device(gpu_id);
+        net::norm_stats_act(static_cast<const bf16 *>(y_dev), n, vox, c, stats_dev, count, gamma_dev, beta_dev, eps,
+                            slope, coef_dev, static_cast<bf16 *>(a_dev), as_stream(stream));
     });
 }
 

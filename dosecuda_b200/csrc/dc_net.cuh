@@ -48,6 +48,9 @@ void conv_wgrad(int mode, const bf16 *p, const bf16 *q, int n, int d, int h, int
 void norm_finalize(const double *stats, int n, int c, long long count, const float *gamma, const float *beta,
                    float eps, float *coef, cudaStream_t s);
 void norm_act(const bf16 *y, int n, long long vox, int c, const float *coef, float slope, bf16 *a, cudaStream_t s);
+void norm_stats_act(const bf16 *y, int n, long long vox, int c, const double *stats, long long count,
+                    const float *gamma, const float *beta, float eps, float slope, float *coef, bf16 *out,
+                    cudaStream_t s);
 void norm_act_bwd(const bf16 *y, const bf16 *da, int n, long long vox, int c, const float *coef,
                   const float *gamma, float slope, double *red, bf16 *dy, float *dgamma, float *dbeta,
                   cudaStream_t s);

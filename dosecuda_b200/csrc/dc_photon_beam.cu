@@ -17,6 +17,8 @@
 // that lattice.
 #include <algorithm>
 #include <cmath>
+#include <cstring>
+#include <iterator>
 #include <string>
 #include <vector>
 
@@ -43,6 +45,9 @@ struct dc_photon_beam {
     float field[4] = {0, 0, 0, 0};  // open-field box at the isocentre plane: x1, x2, y1, y2 (mm)
     bool have_density = false, have_terma = false;
     std::vector<int> probe_host;
+    int lattice = 4;                  // probe lattice stride (0: lines only)
+    PinnedBuffer probe_pin;           // staging of the probe list
+    cudaEvent_t probe_ev = nullptr;   // its last upload
 
     PhotonWork work() {
         PhotonWork w;
@@ -67,6 +72,8 @@ struct dc_photon_beam {
         active.release();
         dirs.release();
         probe.release();
+        if (probe_ev) cudaEventSynchronize(probe_ev), cudaEventDestroy(probe_ev);
+        probe_pin.release();
     }
 };
 
@@ -168,7 +175,11 @@ __global__ void __launch_bounds__(256) gamma_kernel(GammaArgs a) {
 // ---------------------------------------------------------------------------
 // Probe voxels: rays from the source through points of the open field at the
 // isocentre plane (centre, half-field and field-edge positions along both
-// field axes), and lateral profiles across the field at three depths.
+// field axes), lateral profiles across the field at three depths, and a
+// regular lattice of every `lattice`-th voxel along each axis (an unbiased
+// sample of the whole volume; voxels outside the beam cost one texture
+// fetch).  The CCCS of a probe costs about one voxel's march in latency
+// whatever its size, so the lattice is nearly free.
 // ---------------------------------------------------------------------------
 void select_probe(dc_photon_beam &b) {
     const Grid &g = b.g;
@@ -212,7 +223,37 @@ void select_probe(dc_photon_beam &b) {
     }
     std::sort(out.begin(), out.end());
     out.erase(std::unique(out.begin(), out.end()), out.end());
+    if (b.lattice > 0) {
+        const int L = b.lattice, o = L / 2;
+        std::vector<int> lat;
+        lat.reserve((size_t)(g.nx / L + 1) * (g.ny / L + 1) * (g.nz / L + 1));
+        for (int k = o; k < g.nz; k += L)
+            for (int j = o; j < g.ny; j += L)
+                for (int i = o; i < g.nx; i += L) lat.push_back(i + g.nx * (j + g.ny * k));
+        std::vector<int> merged;
+        merged.reserve(out.size() + lat.size());
+        std::merge(out.begin(), out.end(), lat.begin(), lat.end(), std::back_inserter(merged));
+        merged.erase(std::unique(merged.begin(), merged.end()), merged.end());
+        out.swap(merged);
+    }
     b.probe_host.swap(out);
+}
+
+// Selects the probe of the current control point and enqueues its upload on
+// stream s (from pinned staging; no host synchronisation unless the previous
+// upload is still in flight).
+void select_and_upload_probe(dc_photon_beam &b, cudaStream_t s) {
+    select_probe(b);
+    const size_t bytes = b.probe_host.size() * sizeof(int);
+    if (b.probe_ev) DC_CUDA(cudaEventSynchronize(b.probe_ev));
+    else DC_CUDA(cudaEventCreateWithFlags(&b.probe_ev, cudaEventDisableTiming));
+    void *dst = b.probe.ensure(std::max<size_t>(bytes, 256));
+    if (bytes) {
+        void *pin = b.probe_pin.ensure(bytes);
+        std::memcpy(pin, b.probe_host.data(), bytes);
+        DC_CUDA(cudaMemcpyAsync(dst, pin, bytes, cudaMemcpyHostToDevice, s));
+    }
+    DC_CUDA(cudaEventRecord(b.probe_ev, s));
 }
 
 }  // namespace
@@ -308,7 +349,9 @@ int dc_photon_beam_terma(dc_photon_beam *b, const dc_photon_model *model, const 
         DeviceContext &ctx = context(b->device);
         enqueue_terma(ctx, b->g, b->f, b->P, b->C, b->work(), nullptr, terma_out_dev, as_stream(stream));
         b->have_terma = true;
-        b->probe_host.clear();
+        // the probe of this control point, selected on the host while the
+        // TERMA kernels run
+        select_and_upload_probe(*b, as_stream(stream));
     });
 }
 
@@ -324,19 +367,20 @@ int dc_photon_beam_dose(dc_photon_beam *b, float *dose_out_dev, void *stream) {
     });
 }
 
+int dc_photon_beam_probe_config(dc_photon_beam *b, int lattice_stride) {
+    return guarded([&] {
+        need(b != nullptr, "beam must not be NULL.");
+        need(lattice_stride >= 0, "'lattice_stride' must not be negative.");
+        b->lattice = lattice_stride;
+    });
+}
+
 int dc_photon_beam_probe_select(dc_photon_beam *b, int *n_out, void *stream) {
     return guarded([&] {
         need(b != nullptr && n_out != nullptr, "beam and count must not be NULL.");
         need(b->have_terma, "dc_photon_beam_terma must run first.");
-        select_probe(*b);
-        const size_t bytes = b->probe_host.size() * sizeof(int);
         DC_CUDA(cudaSetDevice(b->device));
-        void *dst = b->probe.ensure(std::max<size_t>(bytes, 256));
-        if (bytes) {
-            DC_CUDA(cudaMemcpyAsync(dst, b->probe_host.data(), bytes, cudaMemcpyHostToDevice, as_stream(stream)));
-            // the host vector may change on the next selection
-            DC_CUDA(cudaStreamSynchronize(as_stream(stream)));
-        }
+        select_and_upload_probe(*b, as_stream(stream));
         *n_out = (int)b->probe_host.size();
     });
 }

@@ -446,8 +446,12 @@ class PhotonBeam:
         ptr = C.c_void_p(out.data_ptr()) if out is not None else None
         _lib.raise_for(_lib.load().dc_photon_beam_terma(self._h, C.byref(mv.struct), C.byref(cv.struct), ptr,
                                                          self._s(stream)))
-        self.n_probe = 0
+        self.n_probe = self.probe_voxels(host=False)[1]
         return out
+
+    def probe_config(self, lattice_stride: int):
+        """Probe lattice stride (0: cone lines and profiles only)."""
+        _lib.raise_for(_lib.load().dc_photon_beam_probe_config(self._h, int(lattice_stride)))
 
     def dose(self, out=None, stream=None) -> torch.Tensor:
         if out is None:
@@ -461,13 +465,18 @@ class PhotonBeam:
         self.n_probe = n.value
         return self.n_probe
 
-    def probe_voxels(self) -> tuple[int, int, np.ndarray]:
-        """(device pointer, count, host copy) of the selected probe voxels."""
+    def probe_voxels(self, host: bool = True) -> tuple[int, int, np.ndarray | None]:
+        """(device pointer, count, host copy or None) of the selected probe
+        voxels (selected by ``terma``)."""
         p, n = C.c_void_p(), C.c_int()
-        host = np.empty(max(self.n_probe, 1), np.int32)
-        _lib.raise_for(_lib.load().dc_photon_beam_probe_list(self._h, C.byref(p), C.byref(n),
-                                                              host.ctypes.data_as(C.c_void_p), host.size))
-        return p.value or 0, n.value, host[:n.value]
+        lib = _lib.load()
+        _lib.raise_for(lib.dc_photon_beam_probe_list(self._h, C.byref(p), C.byref(n), None, 0))
+        if not host:
+            return p.value or 0, n.value, None
+        arr = np.empty(max(n.value, 1), np.int32)
+        _lib.raise_for(lib.dc_photon_beam_probe_list(self._h, C.byref(p), C.byref(n), arr.ctypes.data_as(C.c_void_p),
+                                                     arr.size))
+        return p.value or 0, n.value, arr[:n.value]
 
     def probe(self, voxels: torch.Tensor | None = None, out=None, stream=None) -> torch.Tensor:
         """CCCS dose at ``voxels`` (int32 flat indices) or at the selected probe."""

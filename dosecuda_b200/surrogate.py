@@ -142,6 +142,18 @@ class NetOps:
                                                 self._s()))
         return a
 
+    def norm_stats_act(self, y, stats, count, gamma, beta, eps, slope, out=None):
+        """Instance norm from the convolution's statistics + LeakyReLU in one
+        pass; returns (activation, coef)."""
+        n, c = y.shape[0], y.shape[-1]
+        vox = y.numel() // (n * c)
+        a = out if out is not None else torch.empty_like(y)
+        coef = torch.empty((n, c, 4), dtype=torch.float32, device=self.device)
+        _lib.raise_for(self.lib.dc_net_norm_stats_act(self.gpu, _ptr(y), n, vox, c, _ptr(stats), int(count),
+                                                      _ptr(gamma), _ptr(beta), float(eps), float(slope), _ptr(coef),
+                                                      _ptr(a), self._s()))
+        return a, coef
+
     def norm_act_bwd(self, y, da, coef, gamma, slope):
         n, c = y.shape[0], y.shape[-1]
         vox = y.numel() // (n * c)
@@ -284,8 +296,8 @@ class SurrogateNet:
         stats = torch.empty((n, cout, 2), dtype=torch.float64, device=self.device)
         y = ops.conv(CONV3 if kind == "conv3" else DOWN2, x, self._fw[name], cout, stats=stats)
         count = y.shape[1] * y.shape[2] * y.shape[3]
-        coef = ops.norm_finalize(stats, count, self.params[name + ".gamma"], self.params[name + ".beta"], self.eps)
-        a = ops.norm_act(y, coef, self.slope)
+        a, coef = ops.norm_stats_act(y, stats, count, self.params[name + ".gamma"], self.params[name + ".beta"],
+                                     self.eps, self.slope)
         if cache is not None:
             cache[name] = (x, y, coef)
         return a
@@ -420,8 +432,8 @@ def random_phantom_hu(rng: np.random.Generator, shape=(128, 128, 128), spacing=2
 def hu_to_density(hu: torch.Tensor, table_hu, table_density) -> torch.Tensor:
     """Piecewise-linear HU -> relative density with end clamping (the
     np.interp of IMRTDoseGrid.DensityFromHU, plan_imrt.py:114-124)."""
-    xp = torch.as_tensor(np.asarray(table_hu, np.float64), dtype=torch.float64, device=hu.device)
-    fp = torch.as_tensor(np.asarray(table_density, np.float64), dtype=torch.float64, device=hu.device)
+    xp = torch.as_tensor(np.array(table_hu, np.float64), dtype=torch.float64, device=hu.device)
+    fp = torch.as_tensor(np.array(table_density, np.float64), dtype=torch.float64, device=hu.device)
     h = hu.to(torch.float64).clamp(float(xp[0]), float(xp[-1]))
     i = torch.searchsorted(xp, h, right=True).clamp(1, len(xp) - 1)
     x0, x1, f0, f1 = xp[i - 1], xp[i], fp[i - 1], fp[i]
@@ -688,8 +700,7 @@ class PhotonSurrogate:
         self.density.copy_(density)
         self.beam.terma(self.model, cp, out=self.terma, views=views)
         self.run_network()
-        n = self.beam.select_probe()
-        vp, n, _ = self.beam.probe_voxels()
+        vp, n, _ = self.beam.probe_voxels(host=False)  # selected and uploaded by terma
         probe = self.beam.probe()
         probe.mul_(1.0 / scale)  # to the network's units (gamma is scale-free)
         engine.gamma_counts(self.pred, self.grid.spacing, probe, vp, n, 0.0, self.dta, self.dd, self.cutoff,

@@ -149,16 +149,18 @@ def main(argv=None):
         net = SurrogateNet(seed=args.seed, terma_scale=ts, dose_unit=du)
         log("terma_scale %.4g dose_unit %.4g" % (ts, du))
     untrained = SurrogateNet(seed=args.seed, terma_scale=net.terma_scale, dose_unit=net.dose_unit)
-    data = Dataset(maker, range(args.train), dose_unit=net.dose_unit, log=log)
-    t_data = time.time() - t0
-    log("dataset: %d samples in %.1f s" % (len(data), t_data))
-    t1 = time.time()
-    hist = train(net, data, epochs=args.epochs, lr=args.lr, seed=args.seed, log=log, max_steps=args.max_steps,
-                 time_budget_s=args.time_budget, checkpoint=args.out)
-    t_train = time.time() - t1
-    net.save(args.out)
-    del data
-    torch.cuda.empty_cache()
+    hist, t_data, t_train = [], 0.0, 0.0
+    if args.train > 0:  # --train 0 with --init: evaluate the given weights only
+        data = Dataset(maker, range(args.train), dose_unit=net.dose_unit, log=log)
+        t_data = time.time() - t0
+        log("dataset: %d samples in %.1f s" % (len(data), t_data))
+        t1 = time.time()
+        hist = train(net, data, epochs=args.epochs, lr=args.lr, seed=args.seed, log=log, max_steps=args.max_steps,
+                     time_budget_s=args.time_budget, checkpoint=args.out)
+        t_train = time.time() - t1
+        net.save(args.out)
+        del data
+        torch.cuda.empty_cache()
     test_seeds = [TEST_SEED0 + i for i in range(args.test)]
     rows = evaluate(net, maker, test_seeds, accept_rate=args.accept, log=log)
     summ = summarize(rows, args.accept)

@@ -309,9 +309,12 @@ int dc_photon_beam_terma(dc_photon_beam *beam, const dc_photon_model *model, con
                          float *terma_out_dev, void *stream);
 /* Full CCCS dose of the last TERMA (as dc_photon_dose_dev). */
 int dc_photon_beam_dose(dc_photon_beam *beam, float *dose_out_dev, void *stream);
-/* Selects the probe voxels of the last TERMA's control point: rays from
- * the source through the open field's centre, half-field and edge
- * positions, and lateral profiles at three depths.  Synchronous. */
+/* Probe voxels of a control point: rays from the source through the open
+ * field's centre, half-field and edge positions, lateral profiles at three
+ * depths, and every lattice_stride-th voxel along each axis (0: no lattice;
+ * default 4).  dc_photon_beam_terma selects them (on the host, while its
+ * kernels run) and uploads them on its stream; probe_select repeats that. */
+int dc_photon_beam_probe_config(dc_photon_beam *beam, int lattice_stride);
 int dc_photon_beam_probe_select(dc_photon_beam *beam, int *n_out, void *stream);
 /* The selected list: device pointer and count, and optionally a host copy
  * of the first `cap` indices. */
@@ -383,6 +386,11 @@ int dc_net_norm_finalize(int gpu_id, const double *stats_dev, int n, int c, long
 /* a = leaky_relu(coef.x*y + coef.y, slope). */
 int dc_net_norm_act(int gpu_id, const void *y_dev, int n, long long vox, int c, const float *coef_dev, float slope,
                     void *a_dev, void *stream);
+/* dc_net_norm_finalize and dc_net_norm_act in one pass (n <= 16); coef_dev
+ * (or NULL) receives the coefficients for the backward pass. */
+int dc_net_norm_stats_act(int gpu_id, const void *y_dev, int n, long long vox, int c, const double *stats_dev,
+                          long long count, const float *gamma_dev, const float *beta_dev, float eps, float slope,
+                          float *coef_dev, void *a_dev, void *stream);
 /* Backward of norm+activation: dy from da, and dgamma/dbeta (overwritten);
  * red: [n][c][2] double scratch. */
 int dc_net_norm_act_bwd(int gpu_id, const void *y_dev, const void *da_dev, int n, long long vox, int c,
