@@ -617,7 +617,7 @@ def run_surrogate(args, local, dist_mod):
                                "6 MV, gantry 0-355 in 5 deg steps, 2-20 cm MLC fields, 100 MU; held-out seeds "
                                "1000000+i",
                    "network": "4-level 3D encoder-decoder, 16-128 channels, bf16 activations, fp32 accumulation",
-                   "acceptance": "probe gamma(2%/2mm, 10% cutoff) >= 99% on CCCS at ~%d probe voxels"
+                   "acceptance": "probe gamma(2%%/2mm, 10%% cutoff) >= 99%% on CCCS at ~%d probe voxels"
                                  % int(np.mean([r[5] for r in rows])),
                    "l2": "per-beam working set (activations) above the 126 MB L2"},
     }
