@@ -137,6 +137,12 @@ SIGNATURES = {
     "dc_gamma": (C.c_int, [C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_int, _F3, C.c_void_p, C.c_void_p, C.c_longlong,
                            C.c_float, C.c_float, C.c_float, C.c_float, C.c_void_p, C.c_void_p]),
     "dc_net_packed_fragments": (C.c_longlong, [C.c_int, C.c_int, C.c_int]),
+    "dc_net_packed_tc_bytes": (C.c_longlong, [C.c_int, C.c_int]),
+    "dc_net_pack_weights_tc": (C.c_int, [C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
+                                         C.c_void_p, C.c_void_p]),
+    "dc_net_conv_tc": (C.c_int, [C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p,
+                                 C.c_longlong, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "dc_net_tc_error": (C.c_int, [C.c_int, C.POINTER(C.c_int)]),
     "dc_net_pack_weights": (C.c_int, [C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p,
                                       C.c_void_p]),
     "dc_net_conv": (C.c_int, [C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p,

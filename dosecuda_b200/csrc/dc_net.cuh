@@ -62,5 +62,14 @@ void head_loss_bwd(const bf16 *g, long long vox, int c, const float *w, const fl
                    float inv_count, const float *inv_count_dev, double *loss, bf16 *dg, float *dw, float *dbias,
                    cudaStream_t s);
 
+// Tensor-core (tcgen05) 3x3x3 convolution for grids of x extent 128
+// (dc_net_tc.cu): weights prepacked by pack_weights_tc.
+long long packed_tc_bytes(int cin, int cout);
+void pack_weights_tc(const float *master, int taps, int a, int b, int flip, int trans, void *out, cudaStream_t s);
+bool conv_tc_supported(int d, int h, int w, int cin, int cout);
+void conv_tc(const bf16 *x, int n, int d, int h, int w, int cin, const void *wtc, long long wtc_bytes, int cout,
+             bf16 *y, double *stats, cudaStream_t s);
+int take_tc_error();
+
 }  // namespace net
 }  // namespace dc

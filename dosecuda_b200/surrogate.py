@@ -112,6 +112,36 @@ class NetOps:
                                             _ptr(y), _ptr(stats), self._s()))
         return y
 
+    def pack_tc(self, master, flip=0, trans=0, out=None):
+        """Weights packed for the tensor-core (tcgen05) 3x3x3 convolution."""
+        T, A, B = master.shape
+        cin, cout = (B, A) if trans else (A, B)
+        nbytes = self.lib.dc_net_packed_tc_bytes(cin, cout)
+        if nbytes < 0:
+            raise ValueError("no tensor-core convolution for %d -> %d channels" % (cin, cout))
+        if out is None:
+            out = torch.empty(nbytes, dtype=torch.uint8, device=self.device)
+        _lib.raise_for(self.lib.dc_net_pack_weights_tc(self.gpu, _ptr(master), T, A, B, flip, trans, _ptr(out),
+                                                       self._s()))
+        return out
+
+    @staticmethod
+    def tc_supported(shape, cin, cout):
+        d, h, w = shape
+        return w == 128 and d % 2 == 0 and h % 2 == 0 and cout == 16 and cin in (8, 16)
+
+    def conv_tc(self, x, wtc, cout, stats=None, out=None):
+        n, d, h, w, cin = x.shape
+        y = out if out is not None else self._act((n, d, h, w, cout))
+        _lib.raise_for(self.lib.dc_net_conv_tc(self.gpu, _ptr(x), n, d, h, w, cin, _ptr(wtc), wtc.numel(), cout,
+                                               _ptr(y), _ptr(stats), self._s()))
+        return y
+
+    def tc_error(self):
+        flag = C.c_int()
+        _lib.raise_for(self.lib.dc_net_tc_error(self.gpu, C.byref(flag)))
+        return flag.value
+
     def conv_up(self, x, wpk, cout, addend=None, out=None):
         n, d, h, w, cin = x.shape
         y = out if out is not None else self._act((n, 2 * d, 2 * h, 2 * w, cout))
@@ -224,7 +254,8 @@ class SurrogateNet:
         p["head.w"] = torch.randn(16, generator=gen) * 0.1
         p["head.b"] = torch.zeros(1)
         self.params = OrderedDict((k, v.to(self.device, torch.float32).contiguous()) for k, v in p.items())
-        self._fw, self._bw = {}, {}
+        self._fw, self._bw, self._tc = {}, {}, {}
+        self.use_tc = True  # tcgen05 convolutions where the grid allows them
         self.repack()
 
     # -- parameters ----------------------------------------------------------
@@ -241,6 +272,8 @@ class SurrogateNet:
             self._fw[name] = ops.pack(w, ff, ft, out=self._fw.get(name))
             if name != "enc0":
                 self._bw[name] = ops.pack(w, bf, bt, out=self._bw.get(name))
+            if name == "enc0":  # the 8 -> 16 input layer also runs on tcgen05 (x extent 128)
+                self._tc[name] = ops.pack_tc(w, 0, 0, out=self._tc.get(name))
 
     def parameters(self):
         return list(self.params.values())
@@ -294,7 +327,10 @@ class SurrogateNet:
         ops = self.ops
         n = x.shape[0]
         stats = torch.empty((n, cout, 2), dtype=torch.float64, device=self.device)
-        y = ops.conv(CONV3 if kind == "conv3" else DOWN2, x, self._fw[name], cout, stats=stats)
+        if self.use_tc and name in self._tc and ops.tc_supported(tuple(x.shape[1:4]), cin, cout):
+            y = ops.conv_tc(x, self._tc[name], cout, stats=stats)
+        else:
+            y = ops.conv(CONV3 if kind == "conv3" else DOWN2, x, self._fw[name], cout, stats=stats)
         count = y.shape[1] * y.shape[2] * y.shape[3]
         a, coef = ops.norm_stats_act(y, stats, count, self.params[name + ".gamma"], self.params[name + ".beta"],
                                      self.eps, self.slope)

@@ -397,6 +397,22 @@ int dc_net_norm_act_bwd(int gpu_id, const void *y_dev, const void *da_dev, int n
                         const float *coef_dev, const float *gamma_dev, float slope, double *red_dev, void *dy_dev,
                         float *dgamma_dev, float *dbeta_dev, void *stream);
 
+/* The same 3x3x3 convolution on the 5th-generation tensor cores (tcgen05
+ * MMA, fp32 accumulators in tensor memory) for grids of x extent 128 with
+ * even y and z extents, 8->16 or 16->16 channels (the network's
+ * full-resolution layers).  Weights are packed by dc_net_pack_weights_tc
+ * into dc_net_packed_tc_bytes(cin, cout) bytes (-1: unsupported pair);
+ * stats as dc_net_conv. */
+long long dc_net_packed_tc_bytes(int cin, int cout);
+int dc_net_pack_weights_tc(int gpu_id, const float *master_dev, int taps, int a, int b, int flip, int trans,
+                           void *packed_dev, void *stream);
+int dc_net_conv_tc(int gpu_id, const void *x_dev, int n, int d, int h, int w, int cin, const void *wtc_dev,
+                   long long wtc_bytes, int cout, void *y_dev, double *stats_dev, void *stream);
+/* Reads and clears the flag the tensor-core convolution sets when its
+ * bounded wait for the tensor cores expired (that launch's output is not
+ * written).  Synchronous. */
+int dc_net_tc_error(int gpu_id, int *flag);
+
 /* Network input: x8[v] = (terma*terma_scale, density, 0 x 6). */
 int dc_net_pack_input(int gpu_id, const float *terma_dev, const float *density_dev, long long vox, float terma_scale,
                       void *x8_dev, void *stream);

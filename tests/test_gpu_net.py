@@ -325,3 +325,46 @@ def test_network_against_float64_reference(network_case):
     ga = torch.cat([grads[k].detach().double().cpu().reshape(-1) / params[k].grad.norm() for k in params])
     gb = torch.cat([params[k].grad.reshape(-1) / params[k].grad.norm() for k in params])
     assert _cos(ga, gb) > 0.98
+
+
+@pytest.mark.parametrize("cin", [8, 16])
+def test_conv3_tensor_core_forward(ops, cin):
+    """The tcgen05 (TMEM-accumulator) 3x3x3 convolution for x extent 128:
+    against the float64 reference and the mma.sync kernel, with the norm
+    statistics, and without an expired wait."""
+    x, xr = _act((2, 4, 6, 128, cin), 30 + cin)
+    w = R.bf16(_rand((27, cin, 16), 31, 1.0 / np.sqrt(27 * cin)))
+    stats = torch.empty((2, 16, 2), dtype=torch.float64, device="cuda")
+    y = ops.conv_tc(x, ops.pack_tc(w.float().cuda()), 16, stats=stats)
+    torch.cuda.synchronize()
+    assert ops.tc_error() == 0
+    ref = R.ndhwc(F.conv3d(R.ncdhw(xr), R.conv3_weight(w), padding=1))
+    _close(y, ref)
+    yd = y.double().cpu()
+    torch.testing.assert_close(stats[..., 0].cpu(), yd.sum(dim=(1, 2, 3)), rtol=1e-4, atol=1e-3)
+    torch.testing.assert_close(stats[..., 1].cpu(), (yd * yd).sum(dim=(1, 2, 3)), rtol=1e-4, atol=1e-3)
+    y2 = ops.conv(0, x, ops.pack(w.float().cuda()), 16)
+    _close(y, y2.double().cpu())
+    # a second call on the same buffers gives the same result
+    y3 = ops.conv_tc(x, ops.pack_tc(w.float().cuda()), 16)
+    assert torch.equal(y, y3)
+
+
+def test_network_tensor_core_path_matches_mma_path():
+    """On a grid of x extent 128 the full-resolution layers run on tcgen05;
+    the network's features agree with the all-mma.sync network up to the
+    summation-order effects on bf16 roundings."""
+    from dosecuda_b200.surrogate import SurrogateNet
+    net = SurrogateNet(device="cuda", seed=5)
+    shape = (8, 8, 128)
+    gen = torch.Generator().manual_seed(22)
+    terma = (torch.rand(shape, generator=gen) * 2.0).cuda()
+    density = (0.2 + torch.rand(shape, generator=gen)).cuda()
+    x8 = net.ops.pack_input(terma, density, net.terma_scale)
+    net.use_tc = True
+    g_tc = net.features(x8).double().cpu()
+    net.use_tc = False
+    g_mma = net.features(x8).double().cpu()
+    torch.cuda.synchronize()
+    assert net.ops.tc_error() == 0
+    assert _rel_l2(g_tc, g_mma) < 2e-2

@@ -130,3 +130,20 @@ def test_surrogate_phantoms_and_fields():
     assert all(g % 5.0 == 0.0 and 0.0 <= g < 360.0 for g in gantries)
     assert len(set(gantries)) > 50
     assert 2.0 <= min(sides) and max(sides) <= 20.0
+
+
+def test_tensor_core_conv_validates_before_touching_a_gpu():
+    lib = _lib.load()
+    x = np.zeros(64, np.uint16)
+    p = x.ctypes.data_as(V)
+    assert lib.dc_net_packed_tc_bytes(16, 16) == 27 * 2 * 16 * 16
+    assert lib.dc_net_packed_tc_bytes(8, 16) == 18 * 2 * 16 * 16
+    assert lib.dc_net_packed_tc_bytes(32, 32) == -1
+    nb = lib.dc_net_packed_tc_bytes(16, 16)
+    # x extent must be 128, y/z even
+    assert lib.dc_net_conv_tc(0, p, 1, 4, 4, 64, 16, p, nb, 16, p, None, None) == _lib.DC_ERR_VALUE
+    assert lib.dc_net_conv_tc(0, p, 1, 3, 4, 128, 16, p, nb, 16, p, None, None) == _lib.DC_ERR_VALUE
+    assert "x extent 128" in lib.dc_last_error().decode()
+    # packed size must match
+    assert lib.dc_net_conv_tc(0, p, 1, 4, 4, 128, 16, p, nb - 16, 16, p, None, None) == _lib.DC_ERR_VALUE
+    assert lib.dc_net_pack_weights_tc(0, p, 8, 16, 16, 0, 0, p, None) == _lib.DC_ERR_VALUE
