@@ -528,6 +528,63 @@ def run_optimisation(args, local, dist_mod):
     }
 
 
+def vmat_workload(n_cps=18):
+    """The photon workload's phantom with one arc-like beam: n_cps control
+    points of the 10x10 cm field at gantry 0, 20, ..., 100 MU in total."""
+    from dosecuda_b200 import phantoms
+    from dosecuda_b200.plan_imrt import IMRTControlPoint
+    grid, plan = phantoms.photon_small(seed=1)
+    beam = plan.beam_list[0]
+    cp0 = beam.cp_list[0]
+    beam.cp_list = [IMRTControlPoint(cp0.iso, 100.0 / n_cps, np.array(cp0.mlc, copy=True), 360.0 * i / n_cps, 0.0,
+                                     0.0, None, None) for i in range(n_cps)]
+    return grid, plan
+
+
+def run_plan_loop(args, local, dist_mod, dose_kernels_module=None):
+    """IMRT plan of one 18-control-point beam through the plan API: the
+    reference's host loop (HU -> density on the host, one photon_dose_cuda
+    call per control point with host buffers, numpy accumulation) and, for
+    this engine, the device-resident loop (computeIMRTPlan(device=True):
+    HU converted on the GPU, all control points in one call, one copy back).
+    Both give the same dose bit for bit."""
+    import torch
+    from dosecuda_b200 import plan_imrt
+    grid, plan = vmat_workload()
+    saved = plan_imrt.dose_kernels
+    if dose_kernels_module is not None:
+        plan_imrt.dose_kernels = dose_kernels_module
+    try:
+        grid.computeIMRTPlan(plan, gpu_id=local)  # warm-up
+        reps = max(2, min(args.steps, 5))
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            grid.computeIMRTPlan(plan, gpu_id=local)
+        t_host = (time.perf_counter() - t0) * 1e3 / reps
+        host_dose = grid.dose.copy()
+    finally:
+        plan_imrt.dose_kernels = saved
+    out = {"metric": "IMRT plan, 1 beam x 18 control points (128^3): ms per plan",
+           "host_loop_ms": round(t_host, 3), "unit": "ms/plan", "higher_is_better": False,
+           "config": {"workload": "128^3 @ 2.5 mm photon phantom, 18 control points of a 10x10 cm 6 MV field at "
+                                  "gantry 0..340 deg, 100 MU in total"}}
+    if dose_kernels_module is not None:
+        out["value"] = out["host_loop_ms"]
+        return out
+    grid.computeIMRTPlan(plan, gpu_id=local, device=True)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        grid.computeIMRTPlan(plan, gpu_id=local, device=True)
+    t_dev = aggregate_max((time.perf_counter() - t0) * 1e3 / reps, dist_mod)
+    out.update(value=round(t_dev, 3), device_loop_ms=round(t_dev, 3),
+               speedup_vs_host_loop=round(t_host / t_dev, 2),
+               bitwise_equal_to_host_loop=bool(np.array_equal(grid.dose, host_dose)))
+    out["config"]["device_loop"] = "computeIMRTPlan(device=True): HU uploaded once and converted on the GPU, " \
+                                   "the beam's control points in one call, one copy back"
+    return out
+
+
 SURROGATE_WEIGHTS = os.path.join(ROOT, "dosecuda_b200", "weights", "surrogate_6mv.npz")
 
 
@@ -681,6 +738,7 @@ def main_mine(args):
     batched = run_batched(args, local, dist_mod, ws) if args.batch_plans > 0 else None
     optimisation = run_optimisation(args, local, dist_mod) if args.opt_iters > 0 else None
     surrogate = run_surrogate(args, local, dist_mod) if args.surrogate_beams > 0 else None
+    plan_loop = run_plan_loop(args, local, dist_mod) if args.plan_loop else None
     if rank == 0:
         cpu_x = cpu_p = None
         if ws == 1 and not args.no_cpu:
@@ -762,6 +820,7 @@ def main_mine(args):
             "batched": batched,
             "optimisation": optimisation,
             "surrogate": surrogate,
+            "plan_loop": plan_loop,
         }
         print(json.dumps(line))
     if dist_mod is not None:
@@ -846,6 +905,8 @@ def main_reference(args):
                                           "the reference uses spacing[0] on all axes" % (args.batch_plans, len(calls)),
                               "iteration": "one proton_spot_cuda call per beam, WET reused"}}
 
+    plan_loop = run_plan_loop(args, local, None, dose_kernels_module=ref) if args.plan_loop else None
+
     line = {
         "impl": "reference",
         "metric": "CCCS ms/beam",
@@ -874,6 +935,7 @@ def main_reference(args):
                       "higher_is_better": True, "ms_per_step": round(p_s * 1e3, 4),
                       "e2e": {"value": round(n_spots / p_s, 1), "unit": "spots/s"}},
         "batched": batched,
+        "plan_loop": plan_loop,
     }
     print(json.dumps(line))
 
@@ -889,6 +951,8 @@ def main():
     ap.add_argument("--opt-iters", type=int, default=200, help="optimisation iterations (0: skip)")
     ap.add_argument("--tune-cache", action="store_true", help="keep the tile autotuner's JSON cache")
     ap.add_argument("--surrogate-beams", type=int, default=30, help="held-out beams for the surrogate (0: skip)")
+    ap.add_argument("--no-plan-loop", dest="plan_loop", action="store_false",
+                    help="skip the 18-control-point IMRT plan")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -123,6 +123,14 @@ SIGNATURES = {
     "dc_photon_dose": (C.c_int, _VOL + [C.POINTER(PhotonModel), C.POINTER(ControlPoint), C.c_void_p]),
     "dc_photon_dose_dev": (C.c_int, _VOL + [C.POINTER(PhotonModel), C.POINTER(ControlPoint), C.c_void_p,
                                             C.c_void_p]),
+    "dc_hu_convert_dev": (C.c_int, [C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_int,
+                                    C.c_void_p, C.c_void_p]),
+    "dc_proton_raytrace_hu_dev": (C.c_int, [C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_int, _F3, _F3, C.c_void_p,
+                                            C.c_void_p, C.c_int, _F3, C.c_double, C.c_float, C.c_float, C.c_float,
+                                            C.c_void_p, C.c_void_p]),
+    "dc_photon_plan_dose_dev": (C.c_int, [C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_int,
+                                          C.c_int, C.c_int, _F3, _F3, C.POINTER(PhotonModel), C.c_void_p, C.c_int,
+                                          C.c_void_p, C.c_void_p, C.c_void_p]),
     "dc_photon_beam_create": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, _F3, _F3, C.POINTER(C.c_void_p)]),
     "dc_photon_beam_destroy": (C.c_int, [C.c_void_p]),
     "dc_photon_beam_set_density": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),

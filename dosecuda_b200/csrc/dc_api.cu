@@ -273,6 +273,28 @@ int dc_proton_spot_dev(int gpu_id, const float *wet_dev, int nz, int ny, int nx,
 
 // ---------------------------------------------------------------------------
 namespace {
+HuTable make_hu_table(const double *hu, const double *val, int n) {
+    need(hu != nullptr && val != nullptr, "the HU table must not be NULL.");
+    need(n >= 1 && n <= kMaxHuPoints, "the HU table must have between 1 and 64 points.");
+    HuTable t;
+    t.n = n;
+    for (int i = 0; i < n; ++i) {
+        need(std::isfinite(hu[i]) && std::isfinite(val[i]), "HU table entries must be finite.");
+        if (i > 0) need(hu[i] > hu[i - 1], "the HU table must be strictly increasing.");
+        t.hu[i] = hu[i];
+        t.val[i] = val[i];
+    }
+    return t;
+}
+
+// acc = float32(double(acc) + double(d) * w): numpy's float32 += float32 *
+// float64 (the reference's `beam_dose += dose * output_factor`).
+__global__ void accumulate_weighted_kernel(float *__restrict__ acc, const float *__restrict__ d, long long n,
+                                           double w) {
+    for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < n; v += (long long)gridDim.x * blockDim.x)
+        acc[v] = __double2float_rn(__dadd_rn((double)acc[v], __dmul_rn((double)d[v], w)));
+}
+
 void check_photon(const dc_photon_model *m, const dc_control_point *cp) {
     need(m != nullptr && cp != nullptr, "beam model and control point must be given.");
     need(cp->n_mlc_pairs == 0 ||
@@ -336,6 +358,93 @@ int dc_photon_dose_dev(int gpu_id, const float *density_dev, int nz, int ny, int
         ctx.density.ensure(nx, ny, nz, false);
         copy_host_to_array(ctx.density, density_dev, nz, ny, nx, cudaMemcpyDeviceToDevice, s);
         run_photon_pipeline(ctx, g, f, P, C, model->mu_calibration * cp->mu, dose_out_dev, s);
+        ctx.end_call(s);
+    });
+}
+
+// ---------------------------------------------------------------------------
+// HU conversion on the device, fused ray trace, multi-control-point photon
+// plans (SURVEY-ranked next steps of the hot path; no reference counterpart
+// beyond the host loops they replace, plan_impt.py:112-160,
+// plan_imrt.py:114-158).
+// ---------------------------------------------------------------------------
+int dc_hu_convert_dev(int gpu_id, const float *hu_dev, int nz, int ny, int nx, const double *table_hu,
+                      const double *table_val, int n_table, float *out_dev, void *stream) {
+    return guarded([&] {
+        need(hu_dev != nullptr && out_dev != nullptr, "'hu' and the output buffer must not be NULL.");
+        need(nz > 0 && ny > 0 && nx > 0, "'hu' must have positive dimensions.");
+        const HuTable t = make_hu_table(table_hu, table_val, n_table);
+        DeviceContext &ctx = context(gpu_id);
+        (void)ctx;
+        launch_hu_convert(t, hu_dev, nx, ny, nz, out_dev, 0, as_stream(stream));
+    });
+}
+
+int dc_proton_raytrace_hu_dev(int gpu_id, const float *hu_dev, int nz, int ny, int nx, const float spacing[3],
+                              const float origin[3], const double *table_hu, const double *table_rlsp, int n_table,
+                              const float iso[3], double gantry_deg, float couch_deg, float vsadx, float vsady,
+                              float *wet_out_dev, void *stream) {
+    return guarded([&] {
+        check_volume(hu_dev, nz, ny, nx, spacing, origin, "voxel_data");
+        need(iso != nullptr && wet_out_dev != nullptr, "'iso' and the output buffer must be given.");
+        check_proton_model(vsadx, vsady);
+        const HuTable t = make_hu_table(table_hu, table_rlsp, n_table);
+        DeviceContext &ctx = context(gpu_id);
+        std::lock_guard<std::mutex> lk(ctx.mu);
+        cudaStream_t s = as_stream(stream);
+        ctx.begin_call(s);
+        const Grid g = make_grid(nz, ny, nx, spacing);
+        const Frame f = make_frame(iso, origin, gantry_deg, couch_deg, 0.0, (vsadx + vsady) / 2.0f);
+        ctx.density.ensure(nx, ny, nz, true);  // RLSP written straight into the texture array
+        launch_hu_convert(t, hu_dev, nx, ny, nz, nullptr, ctx.density.surf, s);
+        proton_raytrace_core(ctx, g, f, wet_out_dev, s);
+        ctx.end_call(s);
+    });
+}
+
+int dc_photon_plan_dose_dev(int gpu_id, const float *volume_dev, int is_hu, const double *table_hu,
+                            const double *table_density, int n_table, int nz, int ny, int nx, const float spacing[3],
+                            const float origin[3], const dc_photon_model *model, const dc_control_point *cps,
+                            int n_cps, const double *weights, float *dose_accum_dev, void *stream) {
+    return guarded([&] {
+        check_volume(volume_dev, nz, ny, nx, spacing, origin, "voxel_data");
+        need(dose_accum_dev != nullptr, "the output buffer must be given.");
+        need(n_cps >= 0 && (n_cps == 0 || (cps != nullptr && weights != nullptr)),
+             "control points and weights must be given.");
+        HuTable t{};
+        if (is_hu) t = make_hu_table(table_hu, table_density, n_table);
+        static thread_local PhotonParams P;
+        static thread_local CccsCones Cn;
+        for (int q = 0; q < n_cps; ++q) {  // validate every control point before any work
+            check_photon(model, &cps[q]);
+            need(std::isfinite(weights[q]), "control-point weights must be finite.");
+            build_photon_params(*model, cps[q], spacing[0] / 10.0f, P, Cn);
+        }
+        DeviceContext &ctx = context(gpu_id);
+        std::lock_guard<std::mutex> lk(ctx.mu);
+        cudaStream_t s = as_stream(stream);
+        ctx.begin_call(s);
+        const Grid g = make_grid(nz, ny, nx, spacing);
+        if (is_hu) {
+            ctx.density.ensure(nx, ny, nz, true);
+            launch_hu_convert(t, volume_dev, nx, ny, nz, nullptr, ctx.density.surf, s);
+        } else {
+            ctx.density.ensure(nx, ny, nz, false);
+            copy_host_to_array(ctx.density, volume_dev, nz, ny, nx, cudaMemcpyDeviceToDevice, s);
+        }
+        const size_t vb = (size_t)g.n() * sizeof(float);
+        float *cp_dose = static_cast<float *>(ctx.vol_b.ensure(vb));
+        int sms = 0;
+        DC_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx.device));
+        for (int q = 0; q < n_cps; ++q) {
+            build_photon_params(*model, cps[q], spacing[0] / 10.0f, P, Cn);
+            const Frame f = make_frame(cps[q].iso, origin, cps[q].gantry_deg, cps[q].couch_deg,
+                                       cps[q].collimator_deg, model->primary_source_distance);
+            run_photon_pipeline(ctx, g, f, P, Cn, model->mu_calibration * cps[q].mu, cp_dose, s);
+            accumulate_weighted_kernel<<<(unsigned)std::min<long long>((g.n() + 255) / 256, (long long)sms * 8), 256,
+                                         0, s>>>(dose_accum_dev, cp_dose, g.n(), weights[q]);
+            check_launch("accumulate_weighted_kernel");
+        }
         ctx.end_call(s);
     });
 }

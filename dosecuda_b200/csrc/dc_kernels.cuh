@@ -101,4 +101,16 @@ void pencil_beam_batch_tile(int variant, int *threads_y, int *voxels_y);
 void launch_pencil_beam_batch(DeviceContext &ctx, int variant, const PbBatchPlan *plans, const PbBatchBeam *beams,
                               const int2 *items, int n_items, unsigned *next, int lut_len, cudaStream_t s);
 
+// Piecewise-linear HU table (strictly increasing HU), kernel parameter.
+constexpr int kMaxHuPoints = 64;
+struct HuTable {
+    int n;
+    double hu[kMaxHuPoints];
+    double val[kMaxHuPoints];
+};
+// HU -> table value for every voxel: into out (linear, or null) and/or the
+// float cudaArray behind surf (or 0).
+void launch_hu_convert(const HuTable &t, const float *hu, int nx, int ny, int nz, float *out, cudaSurfaceObject_t surf,
+                       cudaStream_t s);
+
 }  // namespace dc

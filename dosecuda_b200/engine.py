@@ -513,3 +513,64 @@ def gamma_counts(eval_dose: torch.Tensor, spacing, ref: torch.Tensor, voxels: to
         C.c_void_p(ref.data_ptr()), count, float(dose_norm), float(dta_mm), float(dd_frac), float(cutoff_frac),
         C.c_void_p(counts.data_ptr()), _stream(eval_dose, stream)))
     return counts
+
+
+def _table(t):
+    th, tv = (np.ascontiguousarray(np.asarray(a, np.float64)) for a in t)
+    if th.ndim != 1 or th.shape != tv.shape:
+        raise ValueError("an HU table is two 1-D arrays of the same length")
+    return th, tv
+
+
+def hu_convert(hu: torch.Tensor, table, out=None, stream=None) -> torch.Tensor:
+    """HU -> table value (relative stopping power or density) on the device;
+    equals np.interp(hu, *table).astype(float32) bit for bit."""
+    _check_volume(hu, "hu")
+    out = _out(hu, out)
+    th, tv = _table(table)
+    nz, ny, nx = hu.shape
+    _lib.raise_for(_lib.load().dc_hu_convert_dev(
+        hu.device.index, C.c_void_p(hu.data_ptr()), nz, ny, nx, th.ctypes.data_as(C.c_void_p),
+        tv.ctypes.data_as(C.c_void_p), th.size, C.c_void_p(out.data_ptr()), _stream(hu, stream)))
+    return out
+
+
+def proton_wet_hu(hu: torch.Tensor, grid, beam, model, table, out=None, stream=None) -> torch.Tensor:
+    """``proton_wet`` from an HU volume: the HU -> RLSP conversion writes the
+    ray tracer's texture directly (no RLSP volume in between)."""
+    _check_volume(hu, "hu")
+    out = _out(hu, out)
+    th, tv = _table(table)
+    nz, ny, nx = hu.shape
+    _lib.raise_for(_lib.load().dc_proton_raytrace_hu_dev(
+        hu.device.index, C.c_void_p(hu.data_ptr()), nz, ny, nx, _spacing(grid), _lib.f3(grid.origin),
+        th.ctypes.data_as(C.c_void_p), tv.ctypes.data_as(C.c_void_p), th.size, _lib.f3(beam.iso),
+        float(beam.gantry_angle), float(beam.couch_angle), float(model.VSADX), float(model.VSADY),
+        C.c_void_p(out.data_ptr()), _stream(hu, stream)))
+    return out
+
+
+def photon_plan_dose(volume: torch.Tensor, grid, model, cps, weights, out: torch.Tensor, hu_table=None, views=None,
+                     stream=None) -> torch.Tensor:
+    """out += sum_i weights[i] * CCCS dose of control point cps[i], in one call
+    (the volume is loaded once; with ``hu_table`` it is an HU volume converted
+    on the device).  weights are float64 (output factors)."""
+    _check_volume(volume, "volume")
+    _check_volume(out, "out")
+    mv = views if views is not None else PhotonModelView(model)
+    cvs = [ControlPointView(cp) for cp in cps]
+    arr = (_lib.ControlPoint * max(len(cvs), 1))(*[c.struct for c in cvs])
+    w = np.ascontiguousarray(np.asarray(weights, np.float64).reshape(-1))
+    if w.size != len(cvs):
+        raise ValueError("one weight per control point is required")
+    if hu_table is not None:
+        th, tv = _table(hu_table)
+        tp = (th.ctypes.data_as(C.c_void_p), tv.ctypes.data_as(C.c_void_p), th.size)
+    else:
+        tp = (None, None, 0)
+    nz, ny, nx = volume.shape
+    _lib.raise_for(_lib.load().dc_photon_plan_dose_dev(
+        volume.device.index, C.c_void_p(volume.data_ptr()), int(hu_table is not None), tp[0], tp[1], tp[2], nz, ny,
+        nx, _spacing(grid), _lib.f3(grid.origin), C.byref(mv.struct), C.cast(arr, C.c_void_p), len(cvs),
+        w.ctypes.data_as(C.c_void_p), C.c_void_p(out.data_ptr()), _stream(volume, stream)))
+    return out

@@ -94,9 +94,16 @@ class IMPTDoseGrid(DoseGrid):
             raise ValueError("Beam model not found for rangeshifter ID %s" % beam.dicom_rangeshifter_label)
         return plan.beam_models[labels.index(beam.dicom_rangeshifter_label)]
 
-    def computeIMPTPlan(self, plan, gpu_id=0):
+    def computeIMPTPlan(self, plan, gpu_id=0, device=False):
         """Dose of every beam: WET ray trace then pencil-beam dose, scaled by
-        the number of fractions (reference plan_impt.py:124-160)."""
+        the number of fractions (reference plan_impt.py:124-160).
+
+        ``device=True`` keeps the plan on the GPU: the HU volume is uploaded
+        once and converted there, straight into the ray tracer's texture;
+        every beam's WET and dose stay on the device and are summed there; the
+        results are copied back once.  Same arithmetic as the host loop."""
+        if device:
+            return self._computeIMPTPlanDevice(plan, gpu_id)
         self.beam_doses = []
         self.dose = np.zeros(self.size, dtype=np.single)
         self.RLSP = self.RLSPFromHU(plan.machine_name)
@@ -109,6 +116,30 @@ class IMPTDoseGrid(DoseGrid):
             self.beam_doses.append(beam_dose * plan.n_fractions)
             self.dose += beam_dose
         self.dose *= plan.n_fractions
+
+    def _computeIMPTPlanDevice(self, plan, gpu_id):
+        import torch
+
+        from . import engine
+        self._check_isotropic()
+        dev = torch.device("cuda", gpu_id)
+        df = pd.read_csv(table_path("protons", plan.machine_name, "HU_RLSP.csv"))
+        table = (df["HU"].to_numpy(), df["RLSP"].to_numpy())
+        hu = torch.as_tensor(np.ascontiguousarray(self.HU, dtype=np.single), device=dev)
+        total = torch.zeros(hu.shape, dtype=torch.float32, device=dev)
+        doses, dmodels = [], {}
+        for beam in plan.beam_list:
+            model = self._model_for(plan, beam)
+            if id(model) not in dmodels:
+                dmodels[id(model)] = engine.ProtonModelDevice(model, device=dev)
+            wet = engine.proton_wet_hu(hu, self, beam, model, table)
+            beam_dose = engine.proton_dose(wet, self, beam, dmodels[id(model)])
+            doses.append(beam_dose * plan.n_fractions)
+            total += beam_dose
+        total *= plan.n_fractions
+        self.RLSP = engine.hu_convert(hu, table).cpu().numpy()
+        self.beam_doses = [d.cpu().numpy() for d in doses]
+        self.dose = total.cpu().numpy()
 
     def computeIMPTWET(self, plan, gpu_id=0):
         """Per-beam smoothed WET volumes, for reuse across spot-weight changes

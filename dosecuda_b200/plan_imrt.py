@@ -89,9 +89,16 @@ class IMRTDoseGrid(DoseGrid):
         df = pd.read_csv(table_path("photons", machine_name, "HU_Density.csv"))
         return np.array(np.interp(self.HU, df["HU"].to_numpy(), df["Density"].to_numpy()), dtype=np.single)
 
-    def computeIMRTPlan(self, plan, gpu_id=0):
+    def computeIMRTPlan(self, plan, gpu_id=0, device=False):
         """Sum over beams and control points of output factor x CCCS dose, times
-        the number of fractions (reference plan_imrt.py:126-158)."""
+        the number of fractions (reference plan_imrt.py:126-158).
+
+        ``device=True`` keeps the plan on the GPU: the HU volume is uploaded
+        once and converted there; each beam's control points run in one call
+        that accumulates output factor x dose on the device; the results are
+        copied back once.  Same arithmetic as the host loop."""
+        if device:
+            return self._computeIMRTPlanDevice(plan, gpu_id)
         self.beam_doses = []
         self.dose = np.zeros(self.size, dtype=np.single)
         self.Density = self.DensityFromHU(plan.machine_name)
@@ -113,6 +120,36 @@ class IMRTDoseGrid(DoseGrid):
             self.beam_doses.append(beam_dose)
             self.dose += beam_dose
         self.dose *= plan.n_fractions
+
+
+    def _computeIMRTPlanDevice(self, plan, gpu_id):
+        import torch
+
+        from . import engine
+        from .dose_kernels import PhotonModelView
+        if self.spacing[0] != self.spacing[1] or self.spacing[0] != self.spacing[2]:
+            raise Exception("Spacing must be isotropic for IMPT dose calculation - consider resampling CT")
+        dev = torch.device("cuda", gpu_id)
+        df = pd.read_csv(table_path("photons", plan.machine_name, "HU_Density.csv"))
+        table = (df["HU"].to_numpy(), df["Density"].to_numpy())
+        hu = torch.as_tensor(np.ascontiguousarray(self.HU, dtype=np.single), device=dev)
+        labels = list(plan.dicom_energy_label.astype(str))
+        total = torch.zeros(hu.shape, dtype=torch.float32, device=dev)
+        doses = []
+        for beam in plan.beam_list:
+            if str(beam.dicom_energy_label) not in labels:
+                raise ValueError("Beam model not found for beam energy %s" % beam.dicom_energy_label)
+            model = plan.beam_models[labels.index(str(beam.dicom_energy_label))]
+            beam_dose = torch.zeros(hu.shape, dtype=torch.float32, device=dev)
+            weights = [float(model.outputFactor(cp)) for cp in beam.cp_list]
+            engine.photon_plan_dose(hu, self, model, beam.cp_list, weights, beam_dose, hu_table=table,
+                                    views=PhotonModelView(model))
+            doses.append(beam_dose)
+            total += beam_dose
+        total *= plan.n_fractions
+        self.Density = engine.hu_convert(hu, table).cpu().numpy()
+        self.beam_doses = [d.cpu().numpy() for d in doses]
+        self.dose = total.cpu().numpy()
 
 
 class IMRTBeam(Beam):

@@ -290,6 +290,32 @@ int dc_photon_dose_dev(int gpu_id,
                        float *dose_out_dev, void *stream);
 
 /* ------------------------------------------------------------------ */
+/* HU conversion on the device and device-resident plan loops.          */
+/* They replace the host-side np.interp conversion and per-beam /        */
+/* per-control-point loops of the plan layer (plan_impt.py:112-160,      */
+/* plan_imrt.py:114-158) with the same arithmetic: the converted volume  */
+/* equals np.interp(...).astype(float32) bit for bit, and the photon     */
+/* accumulation is float32(acc + float64(dose) * weight).  Tables are    */
+/* host arrays of n_table (<= 64) strictly increasing HU and the values. */
+/* ------------------------------------------------------------------ */
+int dc_hu_convert_dev(int gpu_id, const float *hu_dev, int nz, int ny, int nx, const double *table_hu,
+                      const double *table_val, int n_table, float *out_dev, void *stream);
+/* dc_proton_raytrace_dev from an HU volume: HU -> RLSP is written straight
+ * into the ray tracer's texture array, then the WET march + smoothing. */
+int dc_proton_raytrace_hu_dev(int gpu_id, const float *hu_dev, int nz, int ny, int nx, const float spacing[3],
+                              const float origin[3], const double *table_hu, const double *table_rlsp, int n_table,
+                              const float iso[3], double gantry_deg, float couch_deg, float vsadx, float vsady,
+                              float *wet_out_dev, void *stream);
+/* Several control points of one photon beam model in one call: the volume
+ * (relative density, or HU converted with the table when is_hu) is loaded
+ * once; for each control point dose_accum += weights[i] * CCCS dose
+ * (weights: output factors, host doubles).  dose_accum is not cleared. */
+int dc_photon_plan_dose_dev(int gpu_id, const float *volume_dev, int is_hu, const double *table_hu,
+                            const double *table_density, int n_table, int nz, int ny, int nx, const float spacing[3],
+                            const float origin[3], const dc_photon_model *model, const dc_control_point *cps,
+                            int n_cps, const double *weights, float *dose_accum_dev, void *stream);
+
+/* ------------------------------------------------------------------ */
 /* Photon beam kept on the device (surrogate path).  No counterpart in  */
 /* the reference: it splits dc_photon_dose into its TERMA pass and its  */
 /* CCCS pass so that one TERMA serves the surrogate's input, a sparse   */

@@ -147,3 +147,18 @@ def test_tensor_core_conv_validates_before_touching_a_gpu():
     # packed size must match
     assert lib.dc_net_conv_tc(0, p, 1, 4, 4, 128, 16, p, nb - 16, 16, p, None, None) == _lib.DC_ERR_VALUE
     assert lib.dc_net_pack_weights_tc(0, p, 8, 16, 16, 0, 0, p, None) == _lib.DC_ERR_VALUE
+
+
+def test_hu_table_validation_before_touching_a_gpu():
+    lib = _lib.load()
+    x = np.zeros(64, np.float32)
+    p = x.ctypes.data_as(V)
+    th = np.array([-1000.0, 0.0, 0.0, 1000.0])  # not strictly increasing
+    tv = np.array([0.0, 1.0, 1.0, 2.0])
+    assert lib.dc_hu_convert_dev(0, p, 2, 2, 2, th.ctypes.data_as(V), tv.ctypes.data_as(V), 4, p, None) == \
+        _lib.DC_ERR_VALUE
+    assert "increasing" in lib.dc_last_error().decode()
+    th2 = np.linspace(-1000.0, 3000.0, 65)
+    tv2 = np.ones(65)
+    assert lib.dc_hu_convert_dev(0, p, 2, 2, 2, th2.ctypes.data_as(V), tv2.ctypes.data_as(V), 65, p, None) == \
+        _lib.DC_ERR_VALUE
