@@ -771,7 +771,7 @@ def main_mine(args):
                        "parallelism": "replicas" if ws > 1 else "single GPU"},
             "e2e": {"value": round(r["e2e_ms"] / (args.steps * ws), 4), "unit": "ms/beam",
                     "h2d_bytes_per_step": int(r["nvox"] * 4), "d2h_bytes_per_step": int(r["nvox"] * 4),
-                    "api": "dosecuda_b200.dose_kernels.photon_dose_cuda (host numpy in/out, pinned input)"},
+                    "api": "dosecuda_b200.dose_kernels.photon_dose_cuda (host numpy in/out; the input pinned by the caller, the returned array page-locked by the call)"},
             "roofline": {
                 "bound": "fp32",
                 "kernel": "cccs",
