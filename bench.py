@@ -700,6 +700,20 @@ def run_surrogate(args, local, dist_mod):
     }
 
 
+def texture_roof(gpu, achieved_per_s):
+    """CCCS cone samples/s against the texture unit's measured rate of
+    trilinear float2 3D fetches in the same access pattern."""
+    import ctypes as C
+    from dosecuda_b200 import _lib
+    v = C.c_double()
+    rc = _lib.load().dc_texture_fetch_rate(gpu, C.byref(v))
+    if rc != 0:
+        return None
+    return {"achieved": round(achieved_per_s, 1), "peak": round(v.value, 1), "unit": "filtered float2 fetches/s",
+            "frac": round(achieved_per_s / v.value, 4),
+            "peak_kind": "measured (dc_texture_fetch_rate: all SMs, full occupancy, CCCS-like line marches)"}
+
+
 def cpu_baseline_photon():
     """The FP64 C oracle on the host cores: one full control point of the
     photon workload (the whole 128^3 beam; about 10-30 s of CPU time).
@@ -789,6 +803,8 @@ def main_mine(args):
                 # dram__bytes_read.sum + dram__bytes_write.sum of one ncu capture
                 # of this kernel on this workload (profiles/cccs_photon_small.md)
                 "traffic": NCU_TRAFFIC["cccs"],
+                # the binding unit: filtered texture fetches (one per cone sample)
+                "texture": texture_roof(local, r["samples"] / (r["cccs_avg_ms"] * 1e-3)),
             },
             "kernels": {k: {"launches": v[0], "total_ms": round(v[1], 4)} for k, v in r["prof_x"].items()},
             "gpu_launches": x_launch_per_step * args.steps,

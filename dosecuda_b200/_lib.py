@@ -83,6 +83,7 @@ SIGNATURES = {
     "dc_profile_reset": (C.c_int, [C.c_int]),
     "dc_profile_read": (C.c_int, [C.c_int, C.c_int, C.POINTER(C.c_char_p), C.POINTER(C.c_int),
                                   C.POINTER(C.c_double)]),
+    "dc_texture_fetch_rate": (C.c_int, [C.c_int, C.POINTER(C.c_double)]),
     "dc_proton_raytrace": (C.c_int, _VOL + [_F3, C.c_double, C.c_float, C.c_float, C.c_float, C.c_void_p]),
     "dc_proton_raytrace_dev": (C.c_int, _VOL + [_F3, C.c_double, C.c_float, C.c_float, C.c_float, C.c_void_p,
                                                 C.c_void_p]),

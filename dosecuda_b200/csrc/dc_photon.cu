@@ -443,3 +443,76 @@ void run_photon_pipeline(DeviceContext &ctx, const Grid &g, const Frame &f, cons
 }
 
 }  // namespace dc
+
+// ---------------------------------------------------------------------------
+// Texture-unit calibration: the rate of trilinear float2 3D fetches in the
+// CCCS kernel's access pattern (each thread marches a line of samples one
+// voxel apart in a fixed direction; the 32 lanes of a warp start on adjacent
+// voxels), with every fetch used, so that the CCCS's cone-sample rate can be
+// read as a fraction of what the texture unit delivers on this GPU.
+// ---------------------------------------------------------------------------
+namespace dc {
+namespace {
+__global__ void __launch_bounds__(128) texture_rate_kernel(cudaTextureObject_t tex, int n, int steps,
+                                                           float *__restrict__ sink) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const float x0 = (float)(t & 31) + 16.f, y0 = (float)((t >> 5) % 32) + 16.f, z0 = (float)((t >> 10) % 32) + 16.f;
+    const int dir = blockIdx.x % 72;
+    const float th = 0.4f + 0.03f * (float)dir, ph = 0.09f * (float)dir;
+    const float dx = sinf(th) * cosf(ph), dy = sinf(th) * sinf(ph), dz = cosf(th);
+    float acc = 0.f;
+    for (int s = 0; s < steps; ++s) {
+        const float u = (float)(s % 24);
+        const float2 v = tex3D<float2>(tex, fmaf(dx, u, x0), fmaf(dy, u, y0), fmaf(dz, u, z0));
+        acc = fmaf(v.x, v.y, acc);
+    }
+    if (acc == 12345.678f) sink[t] = acc;  // keeps the fetches live
+}
+}  // namespace
+}  // namespace dc
+
+extern "C" int dc_texture_fetch_rate(int gpu_id, double *fetches_per_s) {
+    using namespace dc;
+    return guarded([&] {
+        if (fetches_per_s == nullptr) throw Error(DC_ERR_VALUE, "'fetches_per_s' must not be NULL.");
+        DeviceContext &ctx = context(gpu_id);
+        std::lock_guard<std::mutex> lk(ctx.mu);
+        VolumeArray arr;
+        constexpr int n = 64;
+        arr.ensure(n, n, n, true, 2);
+        cudaStream_t s = ctx.stream;
+        {  // fill with (1, 1)
+            std::vector<float2> host((size_t)n * n * n, make_float2(1.f, 1.f));
+            cudaMemcpy3DParms p{};
+            p.srcPtr = make_cudaPitchedPtr(host.data(), n * sizeof(float2), n, n);
+            p.dstArray = arr.arr;
+            p.extent = make_cudaExtent(n, n, n);
+            p.kind = cudaMemcpyHostToDevice;
+            DC_CUDA(cudaMemcpy3DAsync(&p, s));
+            DC_CUDA(cudaStreamSynchronize(s));
+        }
+        const cudaTextureObject_t tex = arr.texture(0.0f, kAirDensity);
+        int sms = 0, per_sm = 0;
+        DC_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx.device));
+        DC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, texture_rate_kernel, 128, 0));
+        const int blocks = sms * std::max(per_sm, 1);
+        float *sink = static_cast<float *>(ctx.small.ensure((size_t)blocks * 128 * sizeof(float)));
+        const int steps = 4096;
+        texture_rate_kernel<<<blocks, 128, 0, s>>>(tex, n, 64, sink);
+        check_launch("texture_rate_kernel");
+        cudaEvent_t a, b;
+        DC_CUDA(cudaEventCreate(&a));
+        DC_CUDA(cudaEventCreate(&b));
+        DC_CUDA(cudaEventRecord(a, s));
+        texture_rate_kernel<<<blocks, 128, 0, s>>>(tex, n, steps, sink);
+        DC_CUDA(cudaEventRecord(b, s));
+        DC_CUDA(cudaEventSynchronize(b));
+        float ms = 0.f;
+        DC_CUDA(cudaEventElapsedTime(&ms, a, b));
+        cudaEventDestroy(a);
+        cudaEventDestroy(b);
+        check_launch("texture_rate_kernel");
+        arr.release();
+        *fetches_per_s = (double)blocks * 128.0 * steps / (ms * 1e-3);
+    });
+}

@@ -120,6 +120,12 @@ int dc_profile_enable(int gpu_id, int on);
 int dc_profile_reset(int gpu_id);
 int dc_profile_read(int gpu_id, int max, const char **names, int *launches, double *total_ms);
 
+/* Measures the rate of trilinear float2 3D texture fetches the device
+ * delivers in the CCCS kernel's access pattern (all SMs, full occupancy):
+ * the roof of the texture-bound ray-march kernels.  Synchronous, ~1 ms.
+ * No counterpart in the reference. */
+int dc_texture_fetch_rate(int gpu_id, double *fetches_per_s);
+
 /* ------------------------------------------------------------------ */
 /* Proton: water-equivalent thickness (WET) ray trace + BEV smoothing   */
 /* Replaces dose_kernels.proton_raytrace_cuda                           */

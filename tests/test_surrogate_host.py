@@ -162,3 +162,7 @@ def test_hu_table_validation_before_touching_a_gpu():
     tv2 = np.ones(65)
     assert lib.dc_hu_convert_dev(0, p, 2, 2, 2, th2.ctypes.data_as(V), tv2.ctypes.data_as(V), 65, p, None) == \
         _lib.DC_ERR_VALUE
+
+
+def test_texture_calibration_validates_before_touching_a_gpu():
+    assert _lib.load().dc_texture_fetch_rate(0, None) == _lib.DC_ERR_VALUE
