@@ -458,9 +458,10 @@ def run_optimisation(args, local, dist_mod):
     """Differentiable IMPT optimisation: 3 beams, ~7,500 spots; objective
     sum_target (D - 2 Gy)^2 + 10 sum_OAR max(D - 1 Gy, 0)^2 in FP64; gradient
     by the adjoint kernel through torch.autograd; 200 projected-Adam
-    iterations."""
+    iterations (dosecuda_b200.optimize)."""
     import torch
     from dosecuda_b200 import engine, phantoms
+    from dosecuda_b200.optimize import DoseObjective, ImptOptimizer
     from dosecuda_b200.plan_impt import IMPTPlan
     dev = torch.device("cuda", local)
     model = IMPTPlan().beam_models[0]
@@ -479,44 +480,23 @@ def run_optimisation(args, local, dist_mod):
     del X, Y, Z
     plans = [engine.ProtonBeamPlan(grid, bm, model, device=dev) for bm in beams]
     wets = [engine.proton_wet(rl, grid, bm, model) for bm in beams]
-    mus = [p.mu.clone() for p in plans]
-    with torch.no_grad():
-        d0 = sum(p.dose(w, m) for p, w, m in zip(plans, wets, mus))
-        scale = 2.0 / d0.double()[target].mean().item()
-    mu = torch.cat(mus) * scale
-    sizes = [p.n_spots for p in plans]
-
-    def dose_of(m):
-        parts = torch.split(m, sizes)
-        return sum(engine.proton_dose_autograd(q.contiguous(), w, p) for q, w, p in zip(parts, wets, plans))
-
-    def objective(d):
-        d = d.double()
-        return ((d[target] - 2.0) ** 2).sum() + 10.0 * (torch.clamp(d[oar] - 1.0, min=0.0) ** 2).sum()
-
-    mu = mu.detach().requires_grad_(True)
-    opt = torch.optim.Adam([mu], lr=0.02 * mu.detach().mean().item())
-    f0 = objective(dose_of(mu)).item()
+    objective = DoseObjective().uniform(target, 2.0).max_dose(oar, 1.0, weight=10.0)
+    opt = ImptOptimizer(plans, wets, objective)
+    opt.scale_to(target, 2.0)  # mean target dose 2 Gy; lr = 0.02 x the mean weight
+    sizes = opt.sizes
+    f0 = opt.evaluate()
     iters = args.opt_iters
     for _ in range(3):  # warm-up
-        f = objective(dose_of(mu))
-        f.backward()
-        mu.grad = None
+        opt.step()
     torch.cuda.synchronize()
     barrier(dist_mod)
     a, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     a.record()
-    for _ in range(iters):
-        opt.zero_grad(set_to_none=True)
-        f = objective(dose_of(mu))
-        f.backward()
-        opt.step()
-        with torch.no_grad():
-            mu.clamp_(min=0.0)
+    opt.run(iters)
     e.record()
     torch.cuda.synchronize()
     t = aggregate_max(a.elapsed_time(e) / iters, dist_mod)
-    f1 = objective(dose_of(mu)).item()
+    f1 = opt.evaluate()
     return {
         "metric": "IMPT plan optimisation: ms per iteration (dose + adjoint + Adam step)",
         "value": round(t, 3), "unit": "ms/iteration", "higher_is_better": False,

@@ -70,6 +70,7 @@ bool conv_tc_supported(int d, int h, int w, int cin, int cout);
 void conv_tc(const bf16 *x, int n, int d, int h, int w, int cin, const void *wtc, long long wtc_bytes, int cout,
              bf16 *y, double *stats, cudaStream_t s);
 int take_tc_error();
+int tc_wait_selftest(cudaStream_t s);
 
 }  // namespace net
 }  // namespace dc

@@ -105,11 +105,13 @@ struct TcArgs {
     double *stats;
     int d, h;  // grid (x extent is kTcW)
     int tiles_y, tiles_z, n_tiles;
+    long long spin_limit;  // bound of the mbarrier wait
+    int no_mma;            // self-test: issue nothing, so the wait must expire
 };
 
 // Bounded wait for phase `parity` of an mbarrier; false when it expired.
-__device__ __forceinline__ bool wait_mbar(unsigned addr, unsigned parity) {
-    for (long long it = 0; it < kTcSpinLimit; ++it) {
+__device__ __forceinline__ bool wait_mbar(unsigned addr, unsigned parity, long long limit = kTcSpinLimit) {
+    for (long long it = 0; it < limit; ++it) {
         unsigned done;
         asm volatile(
             "{\n\t.reg .pred p;\n\t"
@@ -178,7 +180,7 @@ __global__ void __launch_bounds__(kTcThreads) conv3_tc_kernel(TcArgs a) {
     asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
     const unsigned tmem = *tmem_slot;
 
-    if (tid == 0) {
+    if (tid == 0 && !a.no_mma) {
         const unsigned idesc = instr_desc<N>();
         const unsigned long long adesc0 = smem_desc(su32(sa), S::kPair ? 16u : (unsigned)S::kPlaneBytes, 128);
         const unsigned long long bdesc0 = smem_desc(su32(sb), N * 16, 128);
@@ -207,7 +209,7 @@ __global__ void __launch_bounds__(kTcThreads) conv3_tc_kernel(TcArgs a) {
     }
 
     // bounded wait; every thread votes, so the epilogue decision is uniform
-    const bool done = __syncthreads_and(wait_mbar(su32(mbar), 0) ? 1 : 0) != 0;
+    const bool done = __syncthreads_and(wait_mbar(su32(mbar), 0, a.spin_limit) ? 1 : 0) != 0;
     if (!done && tid == 0) atomicExch(&g_tc_error, 1);
     asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
 
@@ -380,6 +382,7 @@ void conv_tc(const bf16 *x, int n, int d, int h, int w, int cin, const void *wtc
     need(wtc_bytes == packed_tc_bytes(cin, cout), "packed weights do not match the convolution's shape");
     if (stats) DC_CUDA(cudaMemsetAsync(stats, 0, sizeof(double) * 2 * n * cout, s));
     TcArgs a{};
+    a.spin_limit = kTcSpinLimit;
     a.x = x;
     a.w = static_cast<const uint4 *>(wtc);
     a.y = y;
@@ -388,6 +391,41 @@ void conv_tc(const bf16 *x, int n, int d, int h, int w, int cin, const void *wtc
     a.h = h;
     if (cin == 8) return launch_tc<1, 16>(a, n, s);
     return launch_tc<2, 16>(a, n, s);
+}
+
+int take_tc_error();
+
+// Launches one tile with its MMAs withheld and a short wait bound: nothing
+// ever arrives on the CTA's mbarrier, so the bounded wait must expire, set the
+// error flag and skip the epilogue.  Returns the flag (and clears it).
+int tc_wait_selftest(cudaStream_t s) {
+    using S = TcShape<2, 16>;
+    const int d = kTcTZ, h = kTcTY;
+    const size_t xbytes = (size_t)d * h * kTcW * 16 * sizeof(bf16);
+    const size_t ybytes = xbytes;
+    struct Owned {  // frees its allocations on every exit path
+        void *p[3] = {nullptr, nullptr, nullptr};
+        ~Owned() {
+            for (void *q : p) cudaFree(q);
+        }
+    } mem;
+    DC_CUDA(cudaMalloc(&mem.p[0], xbytes));
+    DC_CUDA(cudaMalloc(&mem.p[1], ybytes));
+    DC_CUDA(cudaMalloc(&mem.p[2], S::kBBytes));
+    void *x = mem.p[0], *y = mem.p[1], *w = mem.p[2];
+    DC_CUDA(cudaMemsetAsync(x, 0, xbytes, s));
+    DC_CUDA(cudaMemsetAsync(w, 0, S::kBBytes, s));
+    TcArgs a{};
+    a.x = static_cast<const bf16 *>(x);
+    a.w = static_cast<const uint4 *>(w);
+    a.y = static_cast<bf16 *>(y);
+    a.d = d;
+    a.h = h;
+    a.spin_limit = 256;
+    a.no_mma = 1;
+    launch_tc<2, 16>(a, 1, s);
+    DC_CUDA(cudaStreamSynchronize(s));
+    return take_tc_error();
 }
 
 int take_tc_error() {
@@ -443,6 +481,15 @@ int dc_net_conv_tc(int gpu_id, const void *x_dev, int n, int d, int h, int w, in
         use_device(gpu_id);
         dc::net::conv_tc(static_cast<const dc::net::bf16 *>(x_dev), n, d, h, w, cin, wtc_dev, wtc_bytes, cout,
                          static_cast<dc::net::bf16 *>(y_dev), stats_dev, reinterpret_cast<cudaStream_t>(stream));
+    });
+}
+
+int dc_net_tc_selftest(int gpu_id, int *wait_expired) {
+    return dc::guarded([&] {
+        dc::net::need(wait_expired != nullptr, "'wait_expired' must not be NULL");
+        use_device(gpu_id);
+        dc::net::take_tc_error();  // start from a clear flag
+        *wait_expired = dc::net::tc_wait_selftest(nullptr);
     });
 }
 

@@ -1,4 +1,6 @@
 // dc_runtime.cu — device contexts, cached buffers and textures, profiler.
+#include <atomic>
+#include <cstdlib>
 #include "dc_runtime.cuh"
 #include "dc_common.cuh"
 
@@ -31,9 +33,26 @@ void check_launch(const char *kernel) {
 }
 
 // ---------------------------------------------------------------------------
+// Allocation-failure injection for failure tests: with DC_INJECT_ALLOC_FAIL=N
+// in the environment, the N-th device / pinned / array allocation of the
+// process fails (before the CUDA call) as an out-of-memory would.
+void check_injected_alloc(const char *what) {
+    static const long long fail_at = [] {
+        const char *e = std::getenv("DC_INJECT_ALLOC_FAIL");
+        return e ? std::atoll(e) : 0LL;
+    }();
+    static std::atomic<long long> count{0};
+    if (fail_at <= 0) return;
+    const long long k = ++count;
+    if (k == fail_at)
+        throw Error(DC_ERR_CUDA, std::string("out of memory (injected failure of allocation ") + std::to_string(k) +
+                                     ", " + what + ")");
+}
+
 void *DeviceBuffer::ensure(size_t n) {
     if (n <= bytes && ptr) return ptr;
     release();
+    check_injected_alloc("device buffer");
     size_t want = n < 256 ? 256 : n;
     void *p = nullptr;
     DC_CUDA(cudaMalloc(&p, want));
@@ -51,6 +70,7 @@ void DeviceBuffer::release() {
 void *PinnedBuffer::ensure(size_t n) {
     if (n <= bytes && ptr) return ptr;
     release();
+    check_injected_alloc("pinned host buffer");
     size_t want = n < 4096 ? 4096 : n;
     void *p = nullptr;
     DC_CUDA(cudaMallocHost(&p, want));
@@ -69,6 +89,7 @@ void PinnedBuffer::release() {
 void VolumeArray::ensure(int nx_, int ny_, int nz_, bool want_surface, int channels_) {
     if (arr && nx_ == nx && ny_ == ny && nz_ == nz && channels_ == channels && (surface || !want_surface)) return;
     release();
+    check_injected_alloc("texture array");
     cudaChannelFormatDesc ch = channels_ == 2 ? cudaCreateChannelDesc<float2>() : cudaCreateChannelDesc<float>();
     channels = channels_;
     cudaExtent ext = make_cudaExtent((size_t)nx_, (size_t)ny_, (size_t)nz_);

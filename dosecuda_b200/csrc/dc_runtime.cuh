@@ -13,6 +13,7 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include "../../include/dosecuda.h"
 
@@ -160,18 +161,26 @@ class DeviceContext {
 DeviceContext &context(int device);
 void release_context(int device);
 
-// RAII bracket for a profiled kernel launch on stream s.
+// RAII bracket for a profiled kernel launch on stream s: an NVTX range (the
+// host-side enqueue, visible to any NVTX-aware tracer) and, when the
+// profiler is enabled, CUDA events around the kernel.
 struct KernelTimer {
     DeviceContext &ctx;
     cudaStream_t s;
     cudaEvent_t a = nullptr, b = nullptr;
     KernelTimer(DeviceContext &c, const char *name, cudaStream_t st) : ctx(c), s(st) {
+        nvtxRangePushA(name);
         if (ctx.profiling && !DeviceContext::capturing(s)) ctx.prof_begin(name, s, &a, &b);
     }
     ~KernelTimer() {
         if (b) ctx.prof_end(b, s);
+        nvtxRangePop();
     }
 };
+
+// Throws the injected out-of-memory when DC_INJECT_ALLOC_FAIL selects this
+// allocation (see dc_runtime.cu).
+void check_injected_alloc(const char *what);
 
 // Throws Error(DC_ERR_CUDA) if the last launch failed.
 void check_launch(const char *kernel);

@@ -1,0 +1,205 @@
+"""IMPT spot-weight optimisation on the device, with checkpoint / resume.
+
+The reference has no optimiser: its only affordance is calling
+``proton_raytrace_cuda`` once per beam and ``proton_spot_cuda`` per weight
+change (plan_impt.py:148-155).  Here the WET stays resident, the dose of a
+weight vector is the pencil-beam kernel (``ProtonBeamPlan.dose``) and its
+gradient the hand-written adjoint kernel D^T g (``ProtonBeamPlan.adjoint``)
+behind ``torch.autograd`` (``engine.proton_dose_autograd``).
+
+* ``DoseObjective``: a sum of quadratic voxel terms in float64 -- uniform
+  dose, maximum dose (only the overdose counts), minimum dose (only the
+  underdose counts) -- over voxel sets held as flat index tensors, so that an
+  evaluation never synchronises with the host.
+* ``ImptOptimizer``: projected Adam on the spot weights (weights >= 0 after
+  every step); ``save``/``load`` write and restore the weights, Adam's moments
+  and step count and the iteration, so an interrupted run continues exactly.
+* ``save_influence_csr``/``load_influence_csr``: a dose-influence matrix
+  (``ProtonBeamPlan.influence_csr``) cached as ``.npz``."""
+from __future__ import annotations
+
+import os
+
+import numpy as np
+import torch
+
+from . import engine
+
+
+class DoseObjective:
+    """f(D) = sum_k w_k sum_{v in V_k} r_k(D_v)^2, evaluated in float64, with
+    r = D - d (uniform), max(D - d, 0) (maximum dose) or min(D - d, 0)
+    (minimum dose)."""
+
+    KINDS = ("uniform", "max", "min")
+
+    def __init__(self):
+        self.terms = []
+
+    @staticmethod
+    def _index(mask: torch.Tensor) -> torch.Tensor:
+        if mask.dtype != torch.bool:
+            raise ValueError("a voxel set is a boolean mask of the dose grid")
+        return torch.nonzero(mask.reshape(-1), as_tuple=False).squeeze(1)
+
+    def add(self, kind: str, mask: torch.Tensor, dose: float, weight: float = 1.0) -> "DoseObjective":
+        if kind not in self.KINDS:
+            raise ValueError("term kind must be one of %s" % (self.KINDS,))
+        if weight < 0:
+            raise ValueError("term weights must be non-negative")
+        self.terms.append((kind, self._index(mask), float(dose), float(weight), tuple(mask.shape)))
+        return self
+
+    def uniform(self, mask, dose, weight=1.0):
+        return self.add("uniform", mask, dose, weight)
+
+    def max_dose(self, mask, dose, weight=1.0):
+        return self.add("max", mask, dose, weight)
+
+    def min_dose(self, mask, dose, weight=1.0):
+        return self.add("min", mask, dose, weight)
+
+    def __call__(self, dose: torch.Tensor) -> torch.Tensor:
+        flat = dose.reshape(-1)
+        f = torch.zeros((), dtype=torch.float64, device=dose.device)
+        for kind, idx, d, w, shape in self.terms:
+            if tuple(dose.shape) != shape:
+                raise ValueError("dose has shape %s, the objective's voxel sets %s" % (tuple(dose.shape), shape))
+            r = flat.index_select(0, idx).double() - d
+            if kind == "max":
+                r = torch.clamp(r, min=0.0)
+            elif kind == "min":
+                r = torch.clamp(r, max=0.0)
+            f = f + w * (r * r).sum()
+        return f
+
+
+class ImptOptimizer:
+    """Projected Adam on the spot weights of one or more beams of a plan.
+
+    ``plans``: ``engine.ProtonBeamPlan`` per beam (or any object with the same
+    ``dose``/``adjoint``/``n_spots``/``mu``); ``wets``: each beam's smoothed WET
+    on the dose grid.  The weight vector concatenates the beams' spots in
+    order; ``lr`` defaults to ``lr_frac`` x the mean initial weight."""
+
+    def __init__(self, plans, wets, objective: DoseObjective, mu: torch.Tensor | None = None, lr: float | None = None,
+                 lr_frac: float = 0.02):
+        self.plans, self.wets = list(plans), list(wets)
+        if len(self.plans) != len(self.wets) or not self.plans:
+            raise ValueError("one WET volume per beam is required")
+        self.objective = objective
+        self.sizes = [int(p.n_spots) for p in self.plans]
+        mu0 = torch.cat([p.mu for p in self.plans]) if mu is None else mu
+        if mu0.numel() != sum(self.sizes):
+            raise ValueError("mu must hold one weight per spot of all beams")
+        self.mu = mu0.detach().to(device=self.wets[0].device, dtype=torch.float32).clone().requires_grad_(True)
+        self.lr = float(lr) if lr is not None else float(lr_frac * self.mu.detach().mean().item())
+        self.opt = torch.optim.Adam([self.mu], lr=self.lr)
+        self.iteration = 0
+        self.value = None  # objective (device tensor) at the weights before the last step
+
+    def dose(self, mu: torch.Tensor | None = None) -> torch.Tensor:
+        """Total dose of all beams; differentiable in ``mu`` (default: the
+        current weights)."""
+        m = self.mu if mu is None else mu
+        parts = torch.split(m, self.sizes)
+        total = None
+        for q, w, p in zip(parts, self.wets, self.plans):
+            d = engine.proton_dose_autograd(q.contiguous(), w, p)
+            total = d if total is None else total + d
+        return total
+
+    def evaluate(self) -> float:
+        with torch.no_grad():
+            return float(self.objective(self.dose(self.mu.detach())))
+
+    def scale_to(self, mask: torch.Tensor, dose: float) -> float:
+        """Scales the weights so that the mean dose over ``mask`` is ``dose``
+        (before the first step only); returns the factor."""
+        if self.iteration:
+            raise RuntimeError("scale_to is for the initial weights")
+        with torch.no_grad():
+            d = self.dose(self.mu.detach()).double()
+            mean = float(d.reshape(-1)[mask.reshape(-1)].mean())
+            if not mean > 0:
+                raise ValueError("the initial weights give no dose in the mask")
+            k = dose / mean
+            self.mu.mul_(k)
+        self.lr = self.lr * k
+        for g in self.opt.param_groups:
+            g["lr"] = self.lr
+        return k
+
+    def step(self):
+        """One iteration: dose, objective, adjoint gradient, Adam, projection
+        onto mu >= 0.  Does not synchronise with the host."""
+        self.opt.zero_grad(set_to_none=True)
+        f = self.objective(self.dose())
+        f.backward()
+        self.opt.step()
+        with torch.no_grad():
+            self.mu.clamp_(min=0.0)
+        self.value = f.detach()
+        self.iteration += 1
+
+    def run(self, iterations: int, checkpoint: str | None = None, every: int | None = None, log=None):
+        """``iterations`` steps; with ``checkpoint``, the state is saved every
+        ``every`` iterations (default: at the end only) and at the end."""
+        for _ in range(int(iterations)):
+            self.step()
+            if log and self.iteration % 50 == 0:
+                log("iteration %d objective %.6g" % (self.iteration, float(self.value)))
+            if checkpoint and every and self.iteration % every == 0:
+                self.save(checkpoint)
+        if checkpoint:
+            self.save(checkpoint)
+
+    # -- checkpoint / resume --------------------------------------------------
+    def state_dict(self) -> dict:
+        return {"version": 1, "mu": self.mu.detach().cpu().clone(), "adam": self.opt.state_dict(),
+                "iteration": self.iteration, "sizes": list(self.sizes), "lr": self.lr}
+
+    def load_state_dict(self, sd: dict):
+        if sd.get("version") != 1:
+            raise ValueError("unsupported optimiser checkpoint")
+        if list(sd["sizes"]) != self.sizes:
+            raise ValueError("checkpoint was written for beams of %s spots, this plan has %s" %
+                             (list(sd["sizes"]), self.sizes))
+        with torch.no_grad():
+            self.mu.copy_(sd["mu"].to(self.mu.device))
+        self.opt.load_state_dict(sd["adam"])
+        self.lr = float(sd["lr"])
+        self.iteration = int(sd["iteration"])
+
+    def save(self, path: str):
+        """Written to a temporary file and renamed: an interrupted write
+        leaves the previous checkpoint intact."""
+        tmp = str(path) + ".tmp"
+        torch.save(self.state_dict(), tmp)
+        os.replace(tmp, str(path))
+
+    def load(self, path: str):
+        self.load_state_dict(torch.load(str(path), map_location="cpu", weights_only=True))
+
+
+def save_influence_csr(path: str, row_ptr: torch.Tensor, col: torch.Tensor, val: torch.Tensor, shape, n_spots: int):
+    """Caches a dose-influence matrix (voxel rows of ``shape``, ``n_spots``
+    columns) as ``.npz``."""
+    n_vox = int(np.prod(shape))
+    if row_ptr.numel() != n_vox + 1 or col.numel() != val.numel():
+        raise ValueError("inconsistent CSR arrays")
+    np.savez(path, row_ptr=row_ptr.cpu().numpy(), col=col.cpu().numpy(), val=val.cpu().numpy(),
+             shape=np.asarray(shape, np.int64), n_spots=np.int64(n_spots))
+
+
+def load_influence_csr(path: str, device="cuda"):
+    """(row_ptr, col, val, shape, n_spots) of a cached influence matrix."""
+    with np.load(path) as z:
+        row_ptr, col, val = (torch.as_tensor(z[k]).to(device) for k in ("row_ptr", "col", "val"))
+        shape = tuple(int(v) for v in z["shape"])
+        n_spots = int(z["n_spots"])
+    if row_ptr.dtype != torch.int64 or col.dtype != torch.int32 or val.dtype != torch.float32:
+        raise ValueError("influence matrix arrays have unexpected types")
+    if row_ptr.numel() != int(np.prod(shape)) + 1 or int(row_ptr[-1]) != col.numel():
+        raise ValueError("influence matrix arrays are inconsistent")
+    return row_ptr, col, val, shape, n_spots

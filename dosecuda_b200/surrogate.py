@@ -35,6 +35,7 @@ from __future__ import annotations
 
 import ctypes as C
 import math
+import os
 import time
 from collections import OrderedDict
 
@@ -140,6 +141,13 @@ class NetOps:
     def tc_error(self):
         flag = C.c_int()
         _lib.raise_for(self.lib.dc_net_tc_error(self.gpu, C.byref(flag)))
+        return flag.value
+
+    def tc_selftest(self):
+        """Runs the tensor-core wait self-test (MMAs withheld); 1 when the
+        bounded wait expired and was reported."""
+        flag = C.c_int()
+        _lib.raise_for(self.lib.dc_net_tc_selftest(self.gpu, C.byref(flag)))
         return flag.value
 
     def conv_up(self, x, wpk, cout, addend=None, out=None):
@@ -595,7 +603,8 @@ class Trainer:
         self.loss_sum = torch.zeros((), dtype=torch.float64, device=dev)
         self.use_graph = use_graph
         self.graph = None
-        self.steps = 0
+        self.steps = 0  # steps taken by this training run (restored on resume)
+        self._calls = 0  # steps taken by this instance
 
     def _step(self):
         net = self.net
@@ -607,6 +616,51 @@ class Trainer:
         net.repack()
         self.loss_sum += loss[0]
 
+    def _adam_state(self, p):
+        """Adam's per-parameter state, created here (as the capturable
+        optimiser would on its first step) so that it can be restored in
+        place before any step."""
+        st = self.opt.state[p]
+        if not st:
+            st["step"] = torch.zeros((), dtype=torch.float32, device=p.device)
+            st["exp_avg"] = torch.zeros_like(p, memory_format=torch.preserve_format)
+            st["exp_avg_sq"] = torch.zeros_like(p, memory_format=torch.preserve_format)
+        return st
+
+    def state(self):
+        """Host copy of everything the next step depends on: master weights,
+        Adam's moments and step counts, the learning rate and the running
+        loss sum."""
+        net = self.net
+        adam = {}
+        for k, p in net.params.items():
+            st = self._adam_state(p)
+            adam[k] = {n: st[n].detach().cpu().clone() for n in ("step", "exp_avg", "exp_avg_sq")}
+        return {"params": {k: v.detach().cpu().clone() for k, v in net.params.items()},
+                "meta": [net.slope, net.eps, net.terma_scale, net.dose_unit], "adam": adam,
+                "lr": float(self.lr), "loss_sum": float(self.loss_sum), "steps": self.steps}
+
+    def restore(self, state):
+        """Copies a ``state()`` back into the live tensors (in place, so a
+        captured step graph stays valid) and repacks the weights."""
+        net = self.net
+        if set(state["params"]) != set(net.params):
+            raise ValueError("checkpoint parameters do not match the network")
+        slope, eps, ts, du = (float(v) for v in state["meta"])
+        net.slope, net.eps, net.terma_scale, net.dose_unit = slope, eps, ts, du
+        for k, p in net.params.items():
+            src = state["params"][k]
+            if tuple(src.shape) != tuple(p.shape):
+                raise ValueError("parameter %r has shape %s, expected %s" % (k, tuple(src.shape), tuple(p.shape)))
+            p.data.copy_(src.to(p.device))
+            st = self._adam_state(p)
+            for n in ("step", "exp_avg", "exp_avg_sq"):
+                st[n].copy_(state["adam"][k][n].to(p.device))
+        net.repack()
+        self.lr.fill_(float(state["lr"]))
+        self.loss_sum.fill_(float(state["loss_sum"]))
+        self.steps = int(state["steps"])
+
     def load(self, terma, density, target, inv_count):
         self.terma.copy_(terma)
         self.density.copy_(density)
@@ -615,8 +669,9 @@ class Trainer:
 
     def step(self):
         """One step on the loaded sample."""
-        if self.use_graph and self.graph is None and self.steps >= 3:
-            # capture after three eager steps (Adam's state exists by then)
+        if self.use_graph and self.graph is None and self._calls >= 3:
+            # capture after three eager steps of this instance (Adam's state
+            # and every lazily allocated buffer exist by then)
             side = torch.cuda.Stream(self.net.device)
             side.wait_stream(torch.cuda.current_stream(self.net.device))
             g = torch.cuda.CUDAGraph()
@@ -630,27 +685,90 @@ class Trainer:
         else:
             self._step()
         self.steps += 1
+        self._calls += 1
+
+
+def save_training_state(path, trainer: "Trainer", progress: dict):
+    """Writes a resumable training checkpoint: the trainer's ``state()`` plus
+    the loop's progress (step, epoch, position in the epoch's sample order,
+    the generator state the order was drawn from, the schedule, the log
+    history).  Written to a temporary file and renamed, so an interrupted
+    write leaves the previous checkpoint intact."""
+    blob = {"version": 1, "trainer": trainer.state(), "progress": progress}
+    tmp = str(path) + ".tmp"
+    torch.save(blob, tmp)
+    os.replace(tmp, str(path))
+
+
+def load_training_state(path):
+    blob = torch.load(str(path), map_location="cpu", weights_only=True)
+    if blob.get("version") != 1:
+        raise ValueError("unsupported training checkpoint %r" % str(path))
+    return blob
 
 
 def train(net: SurrogateNet, data: Dataset, epochs=1, lr=1e-3, seed=0, log=None, max_steps=None,
-          time_budget_s=None, checkpoint=None, cosine=True, lr_min=1e-5, use_graph=True):
+          time_budget_s=None, checkpoint=None, cosine=True, lr_min=1e-5, use_graph=True, state_path=None,
+          state_every=None, resume=None, session_steps=None, on_step=None):
     """Adam (lr, cosine-decayed to lr_min over the planned steps when
     ``cosine``) on the squared error of the normalised dose, one sample per
     step, samples shuffled each epoch.  Returns a list of (step, epoch, mean
-    loss of the last log interval, seconds)."""
+    loss of the last log interval, seconds).
+
+    ``checkpoint``: weights (.npz) written at each epoch end.
+    ``state_path``: a resumable training checkpoint written every
+    ``state_every`` steps (default: at each epoch end) and when the loop
+    stops.  ``resume``: such a checkpoint to continue from; the schedule
+    (epochs, lr, lr_min, planned steps, seed) is taken from it, and the loop
+    continues at the same sample of the same epoch order.
+    ``session_steps``: stop after this many steps of this call (a time slice
+    of a longer run; the schedule still spans the planned steps).
+    ``on_step(step, epoch, sample_index, lr)`` is called before each step."""
     tr = Trainer(net, data.maker.shape, lr=lr, use_graph=use_graph)
+    step, last, ep0, pos0 = 0, 0, 0, 0
+    hist = []
     rng = np.random.default_rng(seed)
+    if resume is not None:
+        blob = load_training_state(resume)
+        pr = blob["progress"]
+        if int(pr["n_samples"]) != len(data):
+            raise ValueError("checkpoint was written for %d samples, the dataset has %d" % (pr["n_samples"],
+                                                                                          len(data)))
+        tr.restore(blob["trainer"])
+        epochs, lr, lr_min, cosine = int(pr["epochs"]), float(pr["lr"]), float(pr["lr_min"]), bool(pr["cosine"])
+        max_steps = pr["max_steps"]
+        step, last, ep0, pos0 = int(pr["step"]), int(pr["last"]), int(pr["epoch"]), int(pr["pos"])
+        hist = [tuple(h) for h in pr["hist"]]
+        rng.bit_generator.state = pr["rng_state"]
     total = epochs * len(data)
     if max_steps:
         total = min(total, max_steps)
-    hist = []
-    step, t0, last = 0, time.time(), 0
+    t0 = time.time()
     stop = False
-    for ep in range(epochs):
-        for i in rng.permutation(len(data)):
+    step0 = step
+
+    def progress(ep, pos, rng_state):
+        return {"step": step, "last": last, "epoch": ep, "pos": pos, "rng_state": rng_state, "epochs": epochs,
+                "lr": lr, "lr_min": lr_min, "cosine": cosine, "max_steps": max_steps, "n_samples": len(data),
+                "hist": [list(h) for h in hist]}
+
+    for ep in range(ep0, epochs):
+        rng_state = rng.bit_generator.state  # the order of this epoch is drawn from here
+        order = rng.permutation(len(data))
+        pos = pos0 if ep == ep0 else 0
+        while pos < len(order):
+            if step >= total:  # a resumed run that had already finished
+                stop = True
+                break
+            i = order[pos]
+            pos += 1
+            lr_now = lr
             if cosine:
                 frac = min(step / max(total, 1), 1.0)
-                tr.lr.fill_(lr_min + 0.5 * (lr - lr_min) * (1.0 + math.cos(math.pi * frac)))
+                lr_now = lr_min + 0.5 * (lr - lr_min) * (1.0 + math.cos(math.pi * frac))
+                tr.lr.fill_(lr_now)
+            if on_step:
+                on_step(step, ep, int(i), lr_now)
             tr.load(data.terma[i], data.density[i], data.target[i], data.inv_count[i])
             tr.step()
             step += 1
@@ -662,9 +780,16 @@ def train(net: SurrogateNet, data: Dataset, epochs=1, lr=1e-3, seed=0, log=None,
                 log("step %d epoch %d loss %.4e (%.1f s)" % (step, ep, m, time.time() - t0))
             if step >= total or (time_budget_s and time.time() - t0 > time_budget_s):
                 stop = True
+            if session_steps and step - step0 >= session_steps:
+                stop = True
+            if state_path and (stop or (state_every and step % state_every == 0)):
+                save_training_state(state_path, tr, progress(ep, pos, rng_state))
+            if stop:
                 break
         if checkpoint:
             net.save(checkpoint)
+        if state_path and not state_every and not stop:
+            save_training_state(state_path, tr, progress(ep + 1, 0, rng.bit_generator.state))
         if stop:
             break
     torch.cuda.synchronize(net.device)

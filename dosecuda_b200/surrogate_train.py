@@ -30,7 +30,7 @@ import numpy as np
 import torch
 
 from . import engine
-from .surrogate import Dataset, PhotonSurrogate, SampleMaker, SurrogateNet, train
+from .surrogate import Dataset, PhotonSurrogate, SampleMaker, SurrogateNet, load_training_state, train
 
 TEST_SEED0 = 1_000_000
 
@@ -132,6 +132,9 @@ def main(argv=None):
     ap.add_argument("--accept", type=float, default=0.99, help="probe gamma pass rate to accept")
     ap.add_argument("--out", default="surrogate_6mv.npz")
     ap.add_argument("--init", default=None, help="start from these weights")
+    ap.add_argument("--state", default=None, help="write a resumable training checkpoint here")
+    ap.add_argument("--state-every", type=int, default=None, help="steps between training checkpoints")
+    ap.add_argument("--resume", default=None, help="continue training from this training checkpoint")
     ap.add_argument("--report", default=None)
     ap.add_argument("--seed", type=int, default=0)
     args = ap.parse_args(argv)
@@ -142,7 +145,10 @@ def main(argv=None):
     torch.manual_seed(args.seed)
     maker = SampleMaker()
     t0 = time.time()
-    if args.init:
+    if args.resume:  # scales (and weights, Adam state, schedule) come from the checkpoint
+        meta = load_training_state(args.resume)["trainer"]["meta"]
+        net = SurrogateNet(seed=args.seed, terma_scale=float(meta[2]), dose_unit=float(meta[3]))
+    elif args.init:
         net = SurrogateNet.load(args.init)
     else:
         ts, du = choose_scales(maker, range(TEST_SEED0 * 2, TEST_SEED0 * 2 + 16))
@@ -156,7 +162,8 @@ def main(argv=None):
         log("dataset: %d samples in %.1f s" % (len(data), t_data))
         t1 = time.time()
         hist = train(net, data, epochs=args.epochs, lr=args.lr, seed=args.seed, log=log, max_steps=args.max_steps,
-                     time_budget_s=args.time_budget, checkpoint=args.out)
+                     time_budget_s=args.time_budget, checkpoint=args.out, state_path=args.state,
+                     state_every=args.state_every, resume=args.resume)
         t_train = time.time() - t1
         net.save(args.out)
         del data

@@ -444,6 +444,10 @@ int dc_net_conv_tc(int gpu_id, const void *x_dev, int n, int d, int h, int w, in
  * bounded wait for the tensor cores expired (that launch's output is not
  * written).  Synchronous. */
 int dc_net_tc_error(int gpu_id, int *flag);
+/* Failure self-test of that bounded wait: runs one tile with its MMAs
+ * withheld, so the wait must expire; *wait_expired = 1 when the kernel
+ * detected it and returned (the device stays usable).  Synchronous. */
+int dc_net_tc_selftest(int gpu_id, int *wait_expired);
 
 /* Network input: x8[v] = (terma*terma_scale, density, 0 x 6). */
 int dc_net_pack_input(int gpu_id, const float *terma_dev, const float *density_dev, long long vox, float terma_scale,

@@ -350,6 +350,20 @@ def test_conv3_tensor_core_forward(ops, cin):
     assert torch.equal(y, y3)
 
 
+def test_tensor_core_wait_expires_cleanly(ops):
+    """The self-test withholds the MMAs of one tile: the bounded mbarrier wait
+    must expire, be reported, and leave the context usable for a normal
+    tensor-core convolution right after."""
+    assert ops.tc_selftest() == 1
+    assert ops.tc_error() == 0  # the self-test consumed its flag
+    x, xr = _act((1, 2, 4, 128, 16), 40)
+    w = R.bf16(_rand((27, 16, 16), 41, 1.0 / np.sqrt(27 * 16)))
+    y = ops.conv_tc(x, ops.pack_tc(w.float().cuda()), 16)
+    torch.cuda.synchronize()
+    assert ops.tc_error() == 0
+    _close(y, R.ndhwc(F.conv3d(R.ncdhw(xr), R.conv3_weight(w), padding=1)))
+
+
 def test_network_tensor_core_path_matches_mma_path():
     """On a grid of x extent 128 the full-resolution layers run on tcgen05;
     the network's features agree with the all-mma.sync network up to the
