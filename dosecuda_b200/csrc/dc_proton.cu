@@ -23,7 +23,9 @@
 // result is deterministic.  The spot loop is two exponentials per
 // (voxel, spot) pair on the special-function unit (ex2.approx with the
 // log2(e) factor folded into the per-voxel Gaussian scales) plus ~12 FP32
-// operations, so the kernel is bound by the SFU issue rate.
+// operations.  The FP32 part runs on the paired-lane f32x2 instructions of
+// sm_100 (a thread's two voxels share one issue; same IEEE operations, same
+// bits), which leaves the kernel bound by the SFU rate and instruction issue.
 #include <algorithm>
 #include <cmath>
 #include <string>
@@ -146,6 +148,26 @@ __device__ __forceinline__ bool pb_voxel_layer(const LayerRec &L, const float *s
     o.hs2 = (sigma_ht != 0.0f ? -0.5f / sqr(sigma_ht) : -INFINITY) * kLog2e;
     return true;
 }
+
+// Squared distance from two voxels (packed lanes) to one spot's divergent
+// axis, on the paired-lane FP32 instructions of sm_100 (fma.rn.f32x2 and
+// friends: one issue for both voxels).  Each lane performs exactly the
+// scalar sequence
+//   rx = hx - sx,  ry = hy - sy,  ray2 = fma(rx, rx, fma(ry, ry, hz^2)),
+//   dot = fma(tx, rx, fma(ty, ry, -hz)),  r2 = fma(-dot, dot * inv_t2, ray2)
+// (the negations are moved onto exactly negated operands), so the packed and
+// the scalar forms agree bit for bit.
+__device__ __forceinline__ float2 pb_r2_pair(float2 hx, float2 hy, float2 hz2, float2 nhz, float2 nsx, float2 nsy,
+                                            float2 tx, float2 ty, float2 ninv_t2) {
+    const float2 rx = __fadd2_rn(hx, nsx);
+    const float2 ry = __fadd2_rn(hy, nsy);
+    const float2 ray2 = __ffma2_rn(rx, rx, __ffma2_rn(ry, ry, hz2));
+    const float2 dot = __ffma2_rn(tx, rx, __ffma2_rn(ty, ry, nhz));
+    return __ffma2_rn(dot, __fmul2_rn(dot, ninv_t2), ray2);
+}
+
+__device__ __forceinline__ float2 f2(float v) { return make_float2(v, v); }
+__device__ __forceinline__ float2 exp2_pair(float2 x) { return make_float2(fast_exp2(x.x), fast_exp2(x.y)); }
 
 // Lateral cut-off per layer.  A spot's Gaussians are negligible beyond
 // 6 sigma_ht (exp(-18) = 1.5e-8 of the halo peak); sigma_ht = hypot(sigma_t,
@@ -411,7 +433,40 @@ __device__ __forceinline__ void pb_tile(const Grid &g, const Frame &f, const Pro
             }
             __syncthreads();
             if (cn == 0) continue;
-            if (kMode == kPbDose) {
+            if constexpr (kMode == kPbDose && VY % 2 == 0) {
+                if (!any) continue;
+                // voxels (2p, 2p+1) of the thread share the paired lanes of p
+                constexpr int VP = VY / 2;
+                float2 hxp[VP], hyp[VP], hz2p[VP], nhzp[VP], ps2p[VP], hs2p[VP], accp[VP], acch[VP];
+#pragma unroll
+                for (int p = 0; p < VP; ++p) {
+                    hxp[p] = make_float2(hx[2 * p], hx[2 * p + 1]);
+                    hyp[p] = make_float2(hy[2 * p], hy[2 * p + 1]);
+                    hz2p[p] = make_float2(hz2[2 * p], hz2[2 * p + 1]);
+                    nhzp[p] = make_float2(-hz[2 * p], -hz[2 * p + 1]);
+                    ps2p[p] = make_float2(pv[2 * p].ps2, pv[2 * p + 1].ps2);
+                    hs2p[p] = make_float2(pv[2 * p].hs2, pv[2 * p + 1].hs2);
+                    accp[p] = acch[p] = f2(0.f);
+                }
+#pragma unroll 4
+                for (int q = 0; q < cn; ++q) {
+                    const float4 a = s_spot_a[q];
+                    const float4 b = s_spot_b[q];
+                    const float2 nsx = f2(-a.x), nsy = f2(-a.y), tx = f2(b.x), ty = f2(b.y), nit = f2(-b.z);
+                    const float2 mu = f2(a.z);
+#pragma unroll
+                    for (int p = 0; p < VP; ++p) {
+                        const float2 r2 = pb_r2_pair(hxp[p], hyp[p], hz2p[p], nhzp[p], nsx, nsy, tx, ty, nit);
+                        accp[p] = __ffma2_rn(mu, exp2_pair(__fmul2_rn(ps2p[p], r2)), accp[p]);
+                        acch[p] = __ffma2_rn(mu, exp2_pair(__fmul2_rn(hs2p[p], r2)), acch[p]);
+                    }
+                }
+#pragma unroll
+                for (int p = 0; p < VP; ++p) {
+                    if (act[2 * p]) acc[2 * p] += fmaf(pv[2 * p].pf, accp[p].x, pv[2 * p].hf * acch[p].x);
+                    if (act[2 * p + 1]) acc[2 * p + 1] += fmaf(pv[2 * p + 1].pf, accp[p].y, pv[2 * p + 1].hf * acch[p].y);
+                }
+            } else if constexpr (kMode == kPbDose) {
                 if (!any) continue;
                 float accp[VY], acch[VY];
 #pragma unroll
@@ -441,15 +496,33 @@ __device__ __forceinline__ void pb_tile(const Grid &g, const Frame &f, const Pro
                     const float4 a = s_spot_a[q];
                     const float4 b = s_spot_b[q];
                     float kv[VY];
+                    if constexpr (VY % 2 == 0) {
+                        const float2 nsx = f2(-a.x), nsy = f2(-a.y), tx = f2(b.x), ty = f2(b.y), nit = f2(-b.z);
 #pragma unroll
-                    for (int v = 0; v < VY; ++v) {
-                        const float rx = hx[v] - a.x;
-                        const float ry = hy[v] - a.y;
-                        const float ray2 = fmaf(rx, rx, fmaf(ry, ry, hz2[v]));
-                        const float dot = fmaf(b.x, rx, fmaf(b.y, ry, -hz[v]));
-                        const float r2 = fmaf(-dot, dot * b.z, ray2);
-                        kv[v] = act[v] ? fmaf(pv[v].pf, fast_exp2(pv[v].ps2 * r2), pv[v].hf * fast_exp2(pv[v].hs2 * r2))
-                                       : 0.0f;
+                        for (int p = 0; p < VY / 2; ++p) {
+                            const int v0 = 2 * p, v1 = 2 * p + 1;
+                            const float2 r2 = pb_r2_pair(make_float2(hx[v0], hx[v1]), make_float2(hy[v0], hy[v1]),
+                                                         make_float2(hz2[v0], hz2[v1]), make_float2(-hz[v0], -hz[v1]),
+                                                         nsx, nsy, tx, ty, nit);
+                            const float2 ep = exp2_pair(__fmul2_rn(make_float2(pv[v0].ps2, pv[v1].ps2), r2));
+                            const float2 eh = exp2_pair(__fmul2_rn(make_float2(pv[v0].hs2, pv[v1].hs2), r2));
+                            const float2 k2 = __ffma2_rn(make_float2(pv[v0].pf, pv[v1].pf), ep,
+                                                         __fmul2_rn(make_float2(pv[v0].hf, pv[v1].hf), eh));
+                            kv[v0] = act[v0] ? k2.x : 0.0f;
+                            kv[v1] = act[v1] ? k2.y : 0.0f;
+                        }
+                    } else {
+#pragma unroll
+                        for (int v = 0; v < VY; ++v) {
+                            const float rx = hx[v] - a.x;
+                            const float ry = hy[v] - a.y;
+                            const float ray2 = fmaf(rx, rx, fmaf(ry, ry, hz2[v]));
+                            const float dot = fmaf(b.x, rx, fmaf(b.y, ry, -hz[v]));
+                            const float r2 = fmaf(-dot, dot * b.z, ray2);
+                            kv[v] = act[v] ? fmaf(pv[v].pf, fast_exp2(pv[v].ps2 * r2),
+                                                  pv[v].hf * fast_exp2(pv[v].hs2 * r2))
+                                           : 0.0f;
+                        }
                     }
                     if (kMode == kPbAdjoint) {
                         float c = 0.0f;
