@@ -20,8 +20,12 @@
 //    IMRTClasses.cu:398-399,423-424).
 //  * Leaf pairs whose edges are more than 4.5 source-sigmas from the voxel's
 //    projection give exactly erf = +-1 on both edges, i.e. no transmission;
-//    they are skipped without evaluating erf (open-field cost drops from
-//    4*60*2 erf per voxel to the few pairs under the penumbra).
+//    they are skipped without evaluating erf, and with ascending leaf edges
+//    the pairs that remain form one range found by binary search.  Within
+//    it, erf values of equal arguments are reused: a pair's bottom edge is
+//    the previous pair's top edge, and open fields repeat the leaf x
+//    positions, so the 30 mm scatter source (about 38 pairs in range) costs
+//    about one erf per pair instead of four.
 //  * The TERMA kernel applies the CCCS mask and lists the active voxels; the
 //    CCCS is a persistent grid-stride loop over that list, so every lane of
 //    every warp marches (masked voxels no longer idle lanes).
@@ -47,25 +51,73 @@ namespace dc {
 // ---------------------------------------------------------------------------
 // TERMA
 // ---------------------------------------------------------------------------
+// Scaled erf argument of a leaf edge at y (isocentre plane) seen from a
+// voxel at lateral position py: ((y - py) * div + py) * kinv, as in
+// headTransmission (IMRTClasses.cu:130-142), with the multiply-add fused.
+// Written with explicit round-to-nearest intrinsics, which the compiler
+// neither contracts nor reorders, so that every evaluation — the range
+// search, the pair loop's test, and the erf arguments — is the same
+// function of its inputs.
+__device__ __forceinline__ float edge_pos(float y, float py, float div) {
+    return __fmaf_rn(__fsub_rn(y, py), div, py);
+}
+__device__ __forceinline__ float edge_arg(float y, float py, float div, float kinv) {
+    return __fmul_rn(edge_pos(y, py, div), kinv);
+}
+
 __device__ __forceinline__ float head_transmission(const PhotonParams &P, float3 p, float iso_to_source,
                                                    float source_sigma) {
     const float div = (iso_to_source - p.z) / (P.mlc_distance - p.z);
     const float kinv = 1.0f / (source_sigma * sqrtf(2.f));
     // |edge * kinv| > 4.5 on both edges of the same side => erf terms cancel.
     const float lim = 4.5f;
+    // With the pairs' y edges in ascending order (P.edges_sorted) and a
+    // finite, positive scaling, a1 and a2 below are non-decreasing in q
+    // (every operation is monotone), so the pairs the loop skips as
+    // "a2 < -lim" form a prefix and those skipped as "a1 > lim" a suffix:
+    // two binary searches over the same expression find the loop's range,
+    // and the loop still applies its own test to each pair in it — the same
+    // pairs in the same order as a scan of all pairs.
+    int q0 = 0, q1 = P.n_pairs;
+    if (P.edges_sorted && div > 0.0f && div < INFINITY && kinv > 0.0f && kinv < INFINITY && fabsf(p.y) < INFINITY) {
+        int lo = 0, hi = P.n_pairs;
+        while (lo < hi) {  // first pair with a2 >= -lim
+            const int mid = (lo + hi) >> 1;
+            if (edge_arg(P.mlc_yt[mid], p.y, div, kinv) < -lim) lo = mid + 1; else hi = mid;
+        }
+        q0 = lo;
+        hi = P.n_pairs;
+        while (lo < hi) {  // first pair with a1 > lim
+            const int mid = (lo + hi) >> 1;
+            if (edge_arg(P.mlc_yb[mid], p.y, div, kinv) > lim) hi = mid; else lo = mid + 1;
+        }
+        q1 = lo;
+    }
+    // erf of equal arguments is equal: adjacent pairs share a y edge (the
+    // top of one is the bottom of the next) and open fields repeat the same
+    // leaf x positions, so the last top-edge erf and the last x factor are
+    // reused whenever their inputs are the same floats as before.
+    float cached_y = NAN, cached_erf_y = 0.0f;
+    float cached_xl = NAN, cached_xr = NAN, cached_ex = 0.0f;
     float trans = 0.0f;
-    for (int q = 0; q < P.n_pairs; ++q) {
+    for (int q = q0; q < q1; ++q) {
         const float xl = P.mlc_xl[q], xr = P.mlc_xr[q];
         if (xl == xr) continue;  // closed pair: exposed source X is exactly 0
-        const float e1 = ((P.mlc_yb[q] - p.y) * div) + p.y;
-        const float e2 = ((P.mlc_yt[q] - p.y) * div) + p.y;
-        const float a1 = e1 * kinv, a2 = e2 * kinv;
+        const float yb = P.mlc_yb[q], yt = P.mlc_yt[q];
+        const float a1 = edge_arg(yb, p.y, div, kinv);
+        const float a2 = edge_arg(yt, p.y, div, kinv);
         if ((a1 > lim && a2 > lim) || (a1 < -lim && a2 < -lim)) continue;
-        const float t1 = ((xl - p.x) * div) + p.x;
-        const float t2 = ((xr - p.x) * div) + p.x;
-        const float ex = 0.5f * (erff(t2 * kinv) - erff(t1 * kinv));
-        const float ey = 0.5f * (erff(a2) - erff(a1));
-        trans += ex * ey;
+        if (!(xl == cached_xl && xr == cached_xr)) {
+            cached_ex = 0.5f * (erff(edge_arg(xr, p.x, div, kinv)) - erff(edge_arg(xl, p.x, div, kinv)));
+            cached_xl = xl;
+            cached_xr = xr;
+        }
+        const float erf_b = (yb == cached_y) ? cached_erf_y : erff(a1);
+        const float erf_t = erff(a2);
+        cached_y = yt;
+        cached_erf_y = erf_t;
+        const float ey = 0.5f * (erf_t - erf_b);
+        trans = __fmaf_rn(cached_ex, ey, trans);
     }
     return trans;
 }
@@ -336,6 +388,14 @@ void build_photon_params(const dc_photon_model &m, const dc_control_point &cp, f
         P.mlc_yt[q] = (cp.mlc_y_offset[q] + 0.5f * cp.mlc_y_width[q]) * mlc_scale;
         P.mlc_xl[q] = cp.mlc_x1[q] * mlc_scale;
         P.mlc_xr[q] = cp.mlc_x2[q] * mlc_scale;
+    }
+    // Leaf-pair range search precondition (head_transmission): finite y
+    // edges, bottom <= top within a pair, both ascending across pairs.
+    P.edges_sorted = 1;
+    for (int q = 0; q < P.n_pairs; ++q) {
+        const bool ok = std::isfinite(P.mlc_yb[q]) && std::isfinite(P.mlc_yt[q]) && P.mlc_yb[q] <= P.mlc_yt[q] &&
+                        (q == 0 || (P.mlc_yb[q - 1] <= P.mlc_yb[q] && P.mlc_yt[q - 1] <= P.mlc_yt[q]));
+        if (!ok) P.edges_sorted = 0;
     }
     P.n_prof = m.n_profile_points;
     for (int q = 0; q < m.n_profile_points; ++q) {

@@ -18,6 +18,7 @@ constexpr int kMaxConeSteps = 512;  // summed samples per azimuth over all cones
 struct PhotonParams {
     float psd, ssd, pss, sss, mlc_distance, ssw, ea, esw, efd;
     int n_pairs, n_prof, n_spec;
+    int edges_sorted;  // y edges ascending (enables the leaf-pair range search)
     float mlc_xl[kMaxPairs], mlc_xr[kMaxPairs], mlc_yb[kMaxPairs], mlc_yt[kMaxPairs];
     float prof_r[kMaxProfile], prof_i[kMaxProfile], prof_s[kMaxProfile];
     float spec_mu[kMaxSpectrum], spec_pw[kMaxSpectrum], spec_sw[kMaxSpectrum];

@@ -50,6 +50,12 @@ __global__ void __launch_bounds__(128) wet_march_kernel(Grid g, Frame f, cudaTex
 
 __global__ void __launch_bounds__(128) wet_smooth_kernel(Grid g, Frame f, const float *__restrict__ wet,
                                                          float *__restrict__ wet_s) {
+    // The six direction cosines/sines, evaluated once per block with the same
+    // call the per-voxel loop used to make (identical values).
+    __shared__ float s_dir[2][6];
+    const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+    if (tid < 6) sincosf((float)tid * CUDART_PI_F / 3.0f, &s_dir[0][tid], &s_dir[1][tid]);
+    __syncthreads();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
     const int k = blockIdx.z;
@@ -63,8 +69,7 @@ __global__ void __launch_bounds__(128) wet_smooth_kernel(Grid g, Frame f, const 
     float sum = c;
     int n = 1;
     for (int d = 0; d < 6; ++d) {
-        float s, co;
-        sincosf((float)d * CUDART_PI_F / 3.0f, &s, &co);
+        const float s = s_dir[0][d], co = s_dir[1][d];
         for (float dr = 1.0f; dr < rmax && dr < 10.0f; dr += 1.0f) {
             float3 hc = make_float3(h.x + dr * co, h.y + dr * s, h.z);
             const float3 q = head_to_image<false>(f, hc);
