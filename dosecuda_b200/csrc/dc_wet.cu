@@ -13,7 +13,10 @@
 // voxels (coalesced loads/stores; the 32 rays of a warp march side by side so
 // their texture samples share cache lines), blocks of 32x4 voxels.  The march
 // is bound by the texture unit's trilinear fetch rate, one fetch per 1 mm
-// sample.
+// sample.  The smoothing's nearest-voxel lookups avoid the IEEE division and
+// float-to-int conversion on the special-function unit wherever the result
+// is provably the same (nearest_index), which leaves it bound by issue and
+// gather latency.
 #include "dc_common.cuh"
 #include "dc_runtime.cuh"
 #include "dc_kernels.cuh"
@@ -48,6 +51,28 @@ __global__ void __launch_bounds__(128) wet_march_kernel(Grid g, Frame f, cudaTex
     wet[(long long)i + (long long)g.nx * (j + (long long)g.ny * k)] = wet_sum;
 }
 
+// Nearest voxel index (int)roundf(v / s) of the reference's smoothing
+// (CudaClasses.cuh:112-116: IEEE division, then round half away from zero),
+// without the division and the float-to-int conversion on the common path.
+// With r = RN(1/s), qa = RN(v * r) differs from Q = RN(v / s) by less than
+// |qa| * 2^-22 (two relative roundings of 2^-24 each on r and qa, one on Q).
+// When no half-integer lies within |qa| * 2^-21 of qa, Q and qa round to the
+// same integer, which the magic-number addition (1.5 * 2^23, exact for
+// |qa| < 2^21) delivers as bits of a float.  Otherwise — and for inf/NaN —
+// the reference's expression itself is evaluated, so the index is always
+// exactly the reference's.
+__device__ __forceinline__ int nearest_index(float v, float s, float r) {
+    const float magic = 12582912.0f;  // 1.5 * 2^23
+    const float qa = __fmul_rn(v, r);
+    const float t = __fadd_rn(qa, magic);
+    const float d = fabsf(__fsub_rn(qa, __fsub_rn(t, magic)));  // distance to the nearest integer
+    const float aq = fabsf(qa);
+    if (aq < 2097152.0f && __fsub_rn(0.5f, d) > __fmul_rn(aq, 4.76837158203125e-07f)) {  // 2^-21
+        return __float_as_int(t) - 0x4B400000;
+    }
+    return (int)roundf(v / s);
+}
+
 __global__ void __launch_bounds__(128) wet_smooth_kernel(Grid g, Frame f, const float *__restrict__ wet,
                                                          float *__restrict__ wet_s) {
     // The six direction cosines/sines, evaluated once per block with the same
@@ -66,6 +91,7 @@ __global__ void __launch_bounds__(128) wet_smooth_kernel(Grid g, Frame f, const 
     const float3 h = image_to_head<false>(f, p);
     const float c = __ldg(wet + v);
     const float rmax = c * 10.0f;
+    const float rsx = 1.0f / g.sx, rsy = 1.0f / g.sy, rsz = 1.0f / g.sz;
     float sum = c;
     int n = 1;
     for (int d = 0; d < 6; ++d) {
@@ -73,10 +99,10 @@ __global__ void __launch_bounds__(128) wet_smooth_kernel(Grid g, Frame f, const 
         for (float dr = 1.0f; dr < rmax && dr < 10.0f; dr += 1.0f) {
             float3 hc = make_float3(h.x + dr * co, h.y + dr * s, h.z);
             const float3 q = head_to_image<false>(f, hc);
-            // Nearest voxel (CudaClasses.cuh:112-116): division, as the reference.
-            const int qi = (int)roundf((q.x + f.isox) / g.sx);
-            const int qj = (int)roundf((q.y + f.isoy) / g.sy);
-            const int qk = (int)roundf((q.z + f.isoz) / g.sz);
+            // Nearest voxel (CudaClasses.cuh:112-116).
+            const int qi = nearest_index(q.x + f.isox, g.sx, rsx);
+            const int qj = nearest_index(q.y + f.isoy, g.sy, rsy);
+            const int qk = nearest_index(q.z + f.isoz, g.sz, rsz);
             if ((unsigned)qi < (unsigned)g.nx && (unsigned)qj < (unsigned)g.ny &&
                 (unsigned)qk < (unsigned)g.nz) {
                 sum += __ldg(wet + (long long)qi + (long long)g.nx * (qj + (long long)g.ny * qk));
