@@ -705,8 +705,12 @@ def cpu_baseline_photon():
                                           model, cp.iso, cp.mu, cp.ga, cp.ca, cp.ta, np.ascontiguousarray(cp.mlc),
                                           intermediates=True)
     dt = time.perf_counter() - t0
+    # samples of the radiological-depth march (geometry only: 1 mm steps from
+    # every voxel to the volume's exit towards the source at SAD)
+    _, march = oracle.proton_wet(density, np.asarray(grid.spacing, np.float32)[[0, 0, 0]], grid.origin, cp.iso,
+                                 cp.ga, cp.ta, model.primary_source_distance, model.primary_source_distance)
     return {"value": round(dt * 1e3, 1), "unit": "ms/beam", "cores": oracle.num_threads(), "kind": "port",
-            "sample": "one full control point of the 128^3 photon workload (FP64 C/OpenMP oracle)"}, samples
+            "sample": "one full control point of the 128^3 photon workload (FP64 C/OpenMP oracle)"}, samples, march
 
 
 def cpu_baseline_proton():
@@ -714,14 +718,35 @@ def cpu_baseline_proton():
     grid, model, beam, rlsp = proton_workload()
     sp = np.asarray(grid.spacing, np.float32)[[0, 0, 0]]
     t0 = time.perf_counter()
-    wet, _ = oracle.proton_wet(rlsp, sp, grid.origin, beam.iso, beam.gantry_angle, beam.couch_angle, model.VSADX,
-                               model.VSADY)
+    wet, march = oracle.proton_wet(rlsp, sp, grid.origin, beam.iso, beam.gantry_angle, beam.couch_angle,
+                                   model.VSADX, model.VSADY)
     oracle.proton_dose(wet.astype(np.float32), sp, grid.origin, beam.iso, beam.gantry_angle, beam.couch_angle,
                        model, beam.spot_list)
     dt = time.perf_counter() - t0
     return {"value": round(beam.spot_list.shape[0] / dt, 2), "unit": "spots/s", "cores": oracle.num_threads(),
             "kind": "port",
-            "sample": "one full beam of the 96^3 proton workload (600 spots, FP64 C/OpenMP oracle)"}
+            "sample": "one full beam of the 96^3 proton workload (600 spots, FP64 C/OpenMP oracle)"}, march
+
+
+def stage_rates(prof, nvox, march_samples, fetch_rate):
+    """Per-stage rates of one step from the kernel profile: the march's
+    samples/s (samples counted by the oracle) against the measured texture
+    fetch rate, voxels/s of the per-voxel stages, and the march + smoothing
+    compulsory traffic (4 B read + 4 B write per voxel and pass)."""
+    out = {}
+    for name, (launches, total) in prof.items():
+        ms = total / max(launches, 1)
+        e = {"kernel_ms": round(ms, 4), "voxels_per_s": round(nvox / (ms * 1e-3), 1)}
+        if name == "wet_march" and march_samples:
+            rate = march_samples / (ms * 1e-3)
+            e.update({"samples": int(march_samples), "samples_per_s": round(rate, 1)})
+            if fetch_rate:
+                e["texture_frac"] = round(rate / fetch_rate, 4)
+                e["texture_peak_kind"] = "measured float2 fetch rate (dc_texture_fetch_rate); the march fetches float"
+        if name in ("wet_march", "wet_smooth"):
+            e["hbm_gbs_compulsory"] = round(8.0 * nvox / (ms * 1e-3) / 1e9, 2)
+        out[name] = e
+    return out
 
 
 def main_mine(args):
@@ -735,14 +760,17 @@ def main_mine(args):
     plan_loop = run_plan_loop(args, local, dist_mod) if args.plan_loop else None
     if rank == 0:
         cpu_x = cpu_p = None
+        march_x = march_p = None
         if ws == 1 and not args.no_cpu:
-            cpu_x, oracle_samples = cpu_baseline_photon()
-            cpu_p = cpu_baseline_proton()
+            cpu_x, oracle_samples, march_x = cpu_baseline_photon()
+            cpu_p, march_p = cpu_baseline_proton()
             # algorithmic work counted by the oracle (TERMA > 0.01 voxels x cone samples)
             r["achieved_tf"] *= oracle_samples / max(r["samples"], 1)
             r["samples"] = oracle_samples
         pk = r["pk"]
         hbm = pk.get("hbm_gbs", PEAKS_FALLBACK["hbm_gbs"])
+        tex = texture_roof(local, r["samples"] / (r["cccs_avg_ms"] * 1e-3))
+        fetch_rate = tex["peak"] if tex else None
         x_launch_per_step = 4  # wet_march, terma, cone_dirs, cccs
         p_launch_per_step = 3  # wet_march, wet_smooth, pencil_beam
         line = {
@@ -784,9 +812,10 @@ def main_mine(args):
                 # of this kernel on this workload (profiles/cccs_photon_small.md)
                 "traffic": NCU_TRAFFIC["cccs"],
                 # the binding unit: filtered texture fetches (one per cone sample)
-                "texture": texture_roof(local, r["samples"] / (r["cccs_avg_ms"] * 1e-3)),
+                "texture": tex,
             },
             "kernels": {k: {"launches": v[0], "total_ms": round(v[1], 4)} for k, v in r["prof_x"].items()},
+            "stages": stage_rates(r["prof_x"], r["nvox"], march_x, fetch_rate),
             "gpu_launches": x_launch_per_step * args.steps,
             "clocks": r["clocks"],
             "cpu_baseline": cpu_x,
@@ -810,6 +839,7 @@ def main_mine(args):
                              "pairs_per_s": round(r["pairs"] / (r["pb_avg_ms"] * 1e-3), 1),
                              "kernel_ms": round(r["pb_avg_ms"], 4), "traffic": NCU_TRAFFIC["pencil_beam"]},
                 "kernels": {k: {"launches": v[0], "total_ms": round(v[1], 4)} for k, v in r["prof_p"].items()},
+                "stages": stage_rates(r["prof_p"], r["pnvox"], march_p, fetch_rate),
                 "gpu_launches": p_launch_per_step * args.steps,
                 "cpu_baseline": cpu_p,
             },
