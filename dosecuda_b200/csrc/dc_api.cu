@@ -108,6 +108,15 @@ extern "C" {
 
 const char *dc_last_error(void) { return dc::last_error_cstr(); }
 
+int dc_host_buffer_mapped(int gpu_id, const void *host, unsigned long long bytes, int *mapped) {
+    return guarded([&] {
+        need(mapped != nullptr, "'mapped' must not be NULL.");
+        DeviceContext &ctx = context(gpu_id);
+        std::lock_guard<std::mutex> lk(ctx.mu);
+        *mapped = mapped_host_range(host, (size_t)bytes) != nullptr ? 1 : 0;
+    });
+}
+
 int dc_version(void) { return 100; }
 
 int dc_device_count(void) {
@@ -178,9 +187,12 @@ int dc_proton_raytrace(int gpu_id, const float *rlsp, int nz, int ny, int nx, co
         const Frame f = make_frame(iso, origin, gantry_deg, couch_deg, 0.0, (vsadx + vsady) / 2.0f);
         ctx.density.ensure(nx, ny, nz, false);
         copy_host_to_array(ctx.density, rlsp, nz, ny, nx, cudaMemcpyHostToDevice, s);
-        float *wet_s = static_cast<float *>(ctx.vol_b.ensure((size_t)g.n() * sizeof(float)));
+        const size_t vb = (size_t)g.n() * sizeof(float);
+        // page-locked output: the smoothing kernel stores into it directly
+        float *direct = static_cast<float *>(mapped_host_range(wet_out, vb));
+        float *wet_s = direct ? direct : static_cast<float *>(ctx.vol_b.ensure(vb));
         proton_raytrace_core(ctx, g, f, wet_s, s);
-        DC_CUDA(cudaMemcpyAsync(wet_out, wet_s, (size_t)g.n() * sizeof(float), cudaMemcpyDeviceToHost, s));
+        if (!direct) DC_CUDA(cudaMemcpyAsync(wet_out, wet_s, vb, cudaMemcpyDeviceToHost, s));
         ctx.end_call(s);
         DC_CUDA(cudaStreamSynchronize(s));
     });
@@ -227,19 +239,24 @@ int dc_proton_spot(int gpu_id, const float *wet, int nz, int ny, int nx, const f
         const Grid g = make_grid(nz, ny, nx, spacing);
         const Frame f = make_frame(iso, origin, gantry_deg, couch_deg, 0.0, (vsadx + vsady) / 2.0f);
         const size_t vb = (size_t)g.n() * sizeof(float);
-        float *wet_d = static_cast<float *>(ctx.vol_a.ensure(vb));
-        float *dose_d = static_cast<float *>(ctx.vol_b.ensure(vb));
+        // Page-locked WET / dose buffers are read / written by the pencil beam
+        // in place (each voxel's WET read once per tile, each dose written
+        // once); other buffers go through device copies.
+        const float *wet_direct = static_cast<const float *>(mapped_host_range(wet, vb));
+        float *dose_direct = static_cast<float *>(mapped_host_range(dose_out, vb));
+        float *wet_d = wet_direct ? nullptr : static_cast<float *>(ctx.vol_a.ensure(vb));
+        float *dose_d = dose_direct ? dose_direct : static_cast<float *>(ctx.vol_b.ensure(vb));
         const size_t lb = (size_t)n_energies * lut_len * sizeof(float);
         const size_t lb_al = (lb + 255) & ~(size_t)255;
         char *lut = static_cast<char *>(ctx.lut.ensure(3 * lb_al));
-        DC_CUDA(cudaMemcpyAsync(wet_d, wet, vb, cudaMemcpyHostToDevice, s));
+        if (!wet_direct) DC_CUDA(cudaMemcpyAsync(wet_d, wet, vb, cudaMemcpyHostToDevice, s));
         DC_CUDA(cudaMemcpyAsync(lut, lut_depths, lb, cudaMemcpyHostToDevice, s));
         DC_CUDA(cudaMemcpyAsync(lut + lb_al, lut_sigmas, lb, cudaMemcpyHostToDevice, s));
         DC_CUDA(cudaMemcpyAsync(lut + 2 * lb_al, lut_idds, lb, cudaMemcpyHostToDevice, s));
         proton_spot_core(ctx, g, f, layers, recs, reinterpret_cast<const float *>(lut),
                          reinterpret_cast<const float *>(lut + lb_al), reinterpret_cast<const float *>(lut + 2 * lb_al),
-                         lut_len, wet_d, dose_d, s);
-        DC_CUDA(cudaMemcpyAsync(dose_out, dose_d, vb, cudaMemcpyDeviceToHost, s));
+                         lut_len, wet_direct ? wet_direct : wet_d, dose_d, s);
+        if (!dose_direct) DC_CUDA(cudaMemcpyAsync(dose_out, dose_d, vb, cudaMemcpyDeviceToHost, s));
         ctx.end_call(s);
         DC_CUDA(cudaStreamSynchronize(s));
     });
@@ -330,9 +347,11 @@ int dc_photon_dose(int gpu_id, const float *density, int nz, int ny, int nx, con
         ctx.density.ensure(nx, ny, nz, false);
         copy_host_to_array(ctx.density, density, nz, ny, nx, cudaMemcpyHostToDevice, s);
         const size_t vb = (size_t)g.n() * sizeof(float);
-        float *dose_d = static_cast<float *>(ctx.vol_b.ensure(vb));
+        // page-locked output: TERMA (masked zeros) and CCCS store into it directly
+        float *direct = static_cast<float *>(mapped_host_range(dose_out, vb));
+        float *dose_d = direct ? direct : static_cast<float *>(ctx.vol_b.ensure(vb));
         run_photon_pipeline(ctx, g, f, P, C, model->mu_calibration * cp->mu, dose_d, s);
-        DC_CUDA(cudaMemcpyAsync(dose_out, dose_d, vb, cudaMemcpyDeviceToHost, s));
+        if (!direct) DC_CUDA(cudaMemcpyAsync(dose_out, dose_d, vb, cudaMemcpyDeviceToHost, s));
         ctx.end_call(s);
         DC_CUDA(cudaStreamSynchronize(s));
     });

@@ -1,6 +1,8 @@
 // dc_runtime.cu — device contexts, cached buffers and textures, profiler.
 #include <atomic>
 #include <cstdlib>
+#include <cuda.h>
+
 #include "dc_runtime.cuh"
 #include "dc_common.cuh"
 
@@ -47,6 +49,44 @@ void check_injected_alloc(const char *what) {
     if (k == fail_at)
         throw Error(DC_ERR_CUDA, std::string("out of memory (injected failure of allocation ") + std::to_string(k) +
                                      ", " + what + ")");
+}
+
+namespace {
+using PointerAttrFn = CUresult (*)(void *, CUpointer_attribute, CUdeviceptr);
+
+PointerAttrFn pointer_attr_fn() {
+    static PointerAttrFn fn = [] {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuPointerGetAttribute", &p, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess) {
+            (void)cudaGetLastError();
+            return (PointerAttrFn) nullptr;
+        }
+        return reinterpret_cast<PointerAttrFn>(p);
+    }();
+    return fn;
+}
+}  // namespace
+
+void *mapped_host_range(const void *host, size_t bytes) {
+    if (host == nullptr || bytes == 0) return nullptr;
+    cudaPointerAttributes a{};
+    if (cudaPointerGetAttributes(&a, host) != cudaSuccess) {
+        (void)cudaGetLastError();
+        return nullptr;
+    }
+    if (a.type != cudaMemoryTypeHost || a.devicePointer == nullptr) return nullptr;
+    PointerAttrFn fn = pointer_attr_fn();
+    if (fn == nullptr) return nullptr;
+    CUdeviceptr start = 0;
+    size_t size = 0;
+    const CUdeviceptr d = reinterpret_cast<CUdeviceptr>(a.devicePointer);
+    if (fn(&start, CU_POINTER_ATTRIBUTE_RANGE_START_ADDR, d) != CUDA_SUCCESS ||
+        fn(&size, CU_POINTER_ATTRIBUTE_RANGE_SIZE, d) != CUDA_SUCCESS || size == 0)
+        return nullptr;
+    if (d < start || bytes > size || d - start > size - bytes) return nullptr;
+    return a.devicePointer;
 }
 
 void *DeviceBuffer::ensure(size_t n) {

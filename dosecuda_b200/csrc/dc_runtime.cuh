@@ -182,6 +182,14 @@ struct KernelTimer {
 // allocation (see dc_runtime.cu).
 void check_injected_alloc(const char *what);
 
+// Device address through which kernels on the current device may store into
+// the caller's host buffer [host, host + bytes) directly, or nullptr: the
+// buffer must be page-locked host memory mapped into the device's address
+// space (cudaHostAlloc / cudaHostRegister, e.g. torch's pinned allocator),
+// and the whole range must lie inside the one allocation.  Results written
+// this way cross the bus while the kernel runs instead of in a copy after it.
+void *mapped_host_range(const void *host, size_t bytes);
+
 // Throws Error(DC_ERR_CUDA) if the last launch failed.
 void check_launch(const char *kernel);
 

@@ -103,6 +103,15 @@ typedef struct dc_control_point {
 /* Message of the calling thread's last failed call ("" if none). */
 const char *dc_last_error(void);
 
+/* Whether the host buffer [host, host + bytes) is page-locked memory mapped
+ * into gpu_id's address space as one allocation (cudaHostAlloc /
+ * cudaHostRegister, e.g. torch's pinned allocator).  The host-buffer entry
+ * points (dc_proton_raytrace, dc_proton_spot, dc_photon_dose) let their
+ * kernels read the input WET and write the result in place in such buffers,
+ * so the transfers overlap the kernels instead of following them; other
+ * buffers are copied.  No reference counterpart. */
+int dc_host_buffer_mapped(int gpu_id, const void *host, unsigned long long bytes, int *mapped);
+
 /* ABI version (major*10000 + minor*100 + patch). */
 int dc_version(void);
 
