@@ -274,3 +274,28 @@ def test_plan_api_end_to_end(dk):
     xp.addSquareField("6", 6, 6, mu=50, gantry_angle=90.0, collimator_angle=20.0)
     x.computeIMRTPlan(xp)
     assert x.dose.max() > 0 and len(x.beam_doses) == 2
+
+
+@pytest.mark.parametrize("machine,label", [("ElektaVersaSibAxesse", "6"), ("VarianTrueBeamHF", "10")])
+def test_photon_other_machines_and_energies_vs_oracle(dk, machine, label):
+    """The other photon beam models the reference ships through the same
+    kernels: the Elekta machine (80-pair MLC of 5 mm leaves; its four energy
+    folders hold identical tables in the reference, so one stands for all)
+    and the Varian 10 MV spectrum and kernel.  Engine vs the FP64 oracle on a
+    64^3 phantom, oblique gantry and collimator."""
+    import oracle
+    from dosecuda_b200 import phantoms
+    from dosecuda_b200.plan_imrt import IMRTPlan
+    grid = phantoms.photon_phantom((64, 64, 64), 4.0, seed=11)
+    plan = IMRTPlan(machine)
+    plan.addSquareField(label, 8, 6, mu=100, gantry_angle=30.0, collimator_angle=10.0)
+    labels = list(plan.dicom_energy_label.astype(str))
+    model = plan.beam_models[labels.index(label)]
+    cp = plan.beam_list[0].cp_list[0]
+    vol = phantoms.volume_object(grid, grid.DensityFromHU(machine))
+    d = dk.photon_dose_cuda(model, vol, cp, 0)
+    o, _ = oracle.photon_dose(vol.voxel_data, np.asarray(vol.spacing)[[0, 0, 0]], vol.origin, model, cp.iso, cp.mu,
+                              cp.ga, cp.ca, cp.ta, np.ascontiguousarray(cp.mlc))
+    assert d.max() > 0.1 * o.max() > 0
+    assert dose_diff(d, o) <= TOL
+    assert gamma_pass_rate(d, o, 4.0) >= GAMMA
