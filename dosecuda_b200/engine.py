@@ -574,3 +574,85 @@ def photon_plan_dose(volume: torch.Tensor, grid, model, cps, weights, out: torch
         nx, _spacing(grid), _lib.f3(grid.origin), C.byref(mv.struct), C.cast(arr, C.c_void_p), len(cvs),
         w.ctypes.data_as(C.c_void_p), C.c_void_p(out.data_ptr()), _stream(volume, stream)))
     return out
+
+
+class PhotonPlanBasis:
+    """The control points of one photon beam as a linear dose basis on the
+    device, for segment-weight (fluence) optimisation.
+
+    ``basis[b]`` is the CCCS dose of control point b (``photon_dose`` of
+    ``cps[b]``, before its output factor); the beam's dose for segment
+    weights w is  D(w) = sum_b w_b OF_b basis[b]  (``dose``), with the
+    reference plan loop's float32 += float32 * float64 arithmetic, so w = 1
+    gives the plan loop's beam dose bit for bit.  ``adjoint(g)`` is the exact
+    gradient  d(sum_v g_v D_v)/dw_b = OF_b sum_v g_v basis[b][v]  in float64
+    (hand-written kernels ``dc_basis_combine_dev`` / ``dc_basis_adjoint_dev``).
+    Gradients with respect to leaf positions or beamlet fluence would need
+    the transpose of the collapsed-cone superposition and are not provided.
+    """
+
+    def __init__(self, density: torch.Tensor, grid, model, cps, output_factors=None, views=None):
+        _check_volume(density, "density")
+        self.device = density.device
+        self.shape = tuple(density.shape)
+        self.n = len(cps)
+        if self.n < 1:
+            raise ValueError("at least one control point is required")
+        of = [float(model.outputFactor(cp)) for cp in cps] if output_factors is None else list(output_factors)
+        if len(of) != self.n:
+            raise ValueError("one output factor per control point is required")
+        self.output_factors = torch.tensor(of, dtype=torch.float64, device=self.device)
+        self.basis = torch.empty((self.n,) + self.shape, dtype=torch.float32, device=self.device)
+        mv = views if views is not None else PhotonModelView(model)
+        beam = PhotonBeam(grid, self.shape, device=self.device)
+        try:
+            beam.set_density(density)
+            for b, cp in enumerate(cps):
+                beam.terma(model, cp, views=(mv, ControlPointView(cp)))
+                beam.dose(out=self.basis[b])
+        finally:
+            beam.close()
+
+    def dose(self, weights: torch.Tensor | None = None, out: torch.Tensor | None = None, stream=None) -> torch.Tensor:
+        """Beam dose (float32 volume) for segment weights (default all 1)."""
+        coef = self.output_factors if weights is None else \
+            weights.detach().to(device=self.device, dtype=torch.float64).reshape(-1) * self.output_factors
+        if coef.numel() != self.n:
+            raise ValueError("one weight per control point is required")
+        coef = coef.contiguous()
+        out = torch.zeros(self.shape, dtype=torch.float32, device=self.device) if out is None else out.zero_()
+        _check_volume(out, "out")
+        _lib.raise_for(_lib.load().dc_basis_combine_dev(
+            self.device.index, C.c_void_p(self.basis.data_ptr()), self.n, out.numel(), C.c_void_p(coef.data_ptr()),
+            C.c_void_p(out.data_ptr()), _stream(out, stream)))
+        return out
+
+    def adjoint(self, grad_dose: torch.Tensor, stream=None) -> torch.Tensor:
+        """Gradient with respect to the segment weights (float64, one per
+        control point) of sum_v grad_dose_v D_v."""
+        g = grad_dose.detach().to(device=self.device, dtype=torch.float32).contiguous()
+        if tuple(g.shape) != self.shape:
+            raise ValueError("grad_dose must have the volume's shape")
+        out = torch.empty(self.n, dtype=torch.float64, device=self.device)
+        _lib.raise_for(_lib.load().dc_basis_adjoint_dev(
+            self.device.index, C.c_void_p(self.basis.data_ptr()), self.n, g.numel(), C.c_void_p(g.data_ptr()),
+            C.c_void_p(out.data_ptr()), _stream(g, stream)))
+        return out * self.output_factors
+
+
+class _PhotonBasisFn(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, weights, basis):
+        ctx.basis = basis
+        ctx.w_dtype = weights.dtype
+        return basis.dose(weights)
+
+    @staticmethod
+    def backward(ctx, grad_dose):
+        return ctx.basis.adjoint(grad_dose).to(ctx.w_dtype), None
+
+
+def photon_dose_autograd(weights: torch.Tensor, basis: PhotonPlanBasis) -> torch.Tensor:
+    """Differentiable beam dose in the segment weights of a photon beam:
+    forward is the basis combination, backward the adjoint kernel."""
+    return _PhotonBasisFn.apply(weights, basis)

@@ -112,6 +112,24 @@ const char *dc_last_error(void);
  * buffers are copied.  No reference counterpart. */
 int dc_host_buffer_mapped(int gpu_id, const void *host, unsigned long long bytes, int *mapped);
 
+/* ---- Linear dose basis (segment weights of a photon beam) -------------
+ * No reference counterpart: the reference's plan loop (plan_imrt.py:140-156)
+ * computes each control point's dose and adds it times its output factor.
+ * With those doses kept on the device as basis[b][v] (n_basis volumes of
+ * n_vox floats), the plan dose for any segment weights and its adjoint are:
+ *
+ * dc_basis_combine_dev: out[v] = running acc over b (in order) of
+ *   acc = float32(double(acc) + double(basis[b][v]) * coef[b]), starting
+ *   from out[v]: the plan loop's arithmetic, so coef = output factors gives
+ *   its result bit for bit.  coef_dev: n_basis doubles on the device.
+ * dc_basis_adjoint_dev: grad_out[b] = sum_v grad_dose[v] * basis[b][v] in
+ *   float64 (grad_out_dev: n_basis doubles, overwritten).
+ * Both are asynchronous on `stream` and allocate nothing. */
+int dc_basis_combine_dev(int gpu_id, const float *basis, int n_basis, long long n_vox, const double *coef_dev,
+                         float *out_dev, void *stream);
+int dc_basis_adjoint_dev(int gpu_id, const float *basis, int n_basis, long long n_vox, const float *grad_dose_dev,
+                         double *grad_out_dev, void *stream);
+
 /* ABI version (major*10000 + minor*100 + patch). */
 int dc_version(void);
 
