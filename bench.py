@@ -573,7 +573,7 @@ def run_surrogate(args, local, dist_mod):
     surrogate workload (128^3 @ 2.5 mm, random ellipsoids, random gantry and
     MLC field): per beam the surrogate path (TERMA, network, sparse CCCS
     probe, probe gamma, full CCCS when rejected) against the CCCS path (TERMA
-    + full CCCS), both timed with CUDA events; every network dose judged
+    + full CCCS), both timed with CUDA events; every network dose checked
     against the full CCCS with gamma(2%/2mm)."""
     import torch
     from dosecuda_b200 import engine
@@ -599,7 +599,7 @@ def run_surrogate(args, local, dist_mod):
     torch.cuda.synchronize()
     barrier(dist_mod)
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
-    judge = torch.empty(4, dtype=torch.int32, device=dev)
+    vs_cccs = torch.empty(4, dtype=torch.int32, device=dev)
     rows = []
     for density, cp in cases:
         ev[0].record()
@@ -614,8 +614,8 @@ def run_surrogate(args, local, dist_mod):
         ev[3].record()
         torch.cuda.synchronize()
         dmax = float(cccs.max())
-        engine.gamma_counts(net_dose, maker.grid.spacing, cccs, dose_norm=dmax, counts=judge)
-        e, p = (int(v) for v in judge[:2].cpu())
+        engine.gamma_counts(net_dose, maker.grid.spacing, cccs, dose_norm=dmax, counts=vs_cccs)
+        e, p = (int(v) for v in vs_cccs[:2].cpu())
         rows.append((ev[0].elapsed_time(ev[1]), ev[2].elapsed_time(ev[3]), bool(accepted), rate, p / max(e, 1),
                      n_probe))
     t_sur = aggregate_max(float(np.mean([r[0] for r in rows])), dist_mod)
@@ -656,10 +656,10 @@ def run_surrogate(args, local, dist_mod):
         "ms_per_beam_surrogate_path": round(t_sur, 4), "ms_per_beam_cccs_path": round(t_cccs, 4),
         "ms_per_beam_accepted": round(float(np.mean([r[0] for r in acc])), 4) if acc else None,
         "beams": len(rows), "accepted_frac": round(len(acc) / len(rows), 4),
-        "judge_pass_mean_accepted": round(float(np.mean([r[4] for r in acc])), 5) if acc else None,
-        "judge_pass_min_accepted": round(float(np.min([r[4] for r in acc])), 5) if acc else None,
+        "gamma_vs_cccs_mean_accepted": round(float(np.mean([r[4] for r in acc])), 5) if acc else None,
+        "gamma_vs_cccs_min_accepted": round(float(np.min([r[4] for r in acc])), 5) if acc else None,
         "false_accepts": int(sum(1 for r in acc if r[4] < 0.99)),
-        "judge_pass_mean_all": round(float(np.mean([r[4] for r in rows])), 5),
+        "gamma_vs_cccs_mean_all": round(float(np.mean([r[4] for r in rows])), 5),
         "probe_points_mean": round(float(np.mean([r[5] for r in rows])), 1),
         "network_forward_ms": round(t_net, 4),
         "roofline": {"bound": "tensor", "kernel": "conv_gather_kernel 16->16 3x3x3 @ 128^3 (bf16 mma.sync)",

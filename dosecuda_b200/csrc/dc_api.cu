@@ -383,7 +383,7 @@ int dc_photon_dose_dev(int gpu_id, const float *density_dev, int nz, int ny, int
 
 // ---------------------------------------------------------------------------
 // HU conversion on the device, fused ray trace, multi-control-point photon
-// plans (SURVEY-ranked next steps of the hot path; no reference counterpart
+// plans (the next steps either side of the hot path; no reference counterpart
 // beyond the host loops they replace, plan_impt.py:112-160,
 // plan_imrt.py:114-158).
 // ---------------------------------------------------------------------------

@@ -13,9 +13,9 @@ backward) with Adam on the fp32 master weights, one phantom per step.
 
 The evaluation runs ``PhotonSurrogate`` on every test phantom (TERMA ->
 network -> sparse CCCS probe -> probe gamma -> accept or full CCCS) and
-judges every output against the full CCCS dose with gamma(2 %/2 mm, 10 %
+checks every output against the full CCCS dose with gamma(2 %/2 mm, 10 %
 cutoff, global max of the CCCS dose).  It reports the acceptance rate, the
-judged pass rates of accepted beams, the time per beam of the surrogate path
+gamma pass rates (vs CCCS) of accepted beams, the time per beam of the surrogate path
 (fallbacks included) and of the CCCS path, and the same acceptance for the
 untrained network (what training gains over the method without it).
 """
@@ -50,7 +50,7 @@ def choose_scales(maker: SampleMaker, seeds):
 def evaluate(net: SurrogateNet, maker: SampleMaker, seeds, accept_rate=0.99, log=None, time_it=True):
     """Accept/fallback results and timings on the given phantoms."""
     sur = PhotonSurrogate(net, maker.grid, maker.shape, maker.model, accept_rate=accept_rate)
-    judge_counts = torch.empty(4, dtype=torch.int32, device=net.device)
+    cccs_counts = torch.empty(4, dtype=torch.int32, device=net.device)
     rows = []
     ev_a, ev_b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     if seeds:  # warm up (the network's CUDA graph is captured on the second call)
@@ -77,7 +77,7 @@ def evaluate(net: SurrogateNet, maker: SampleMaker, seeds, accept_rate=0.99, log
         net_dose = sur.pred.clone()
         if not accepted:  # pred is in network units when rejected
             net_dose.mul_(maker.dose_scale(cp))
-        # CCCS path (the method without the surrogate) and the judge
+        # CCCS path (the method without the surrogate) and the reference dose
         ev_a.record()
         maker.beam.set_density(density)
         maker.beam.terma(maker.model, cp, views=maker.views(cp))
@@ -86,18 +86,18 @@ def evaluate(net: SurrogateNet, maker: SampleMaker, seeds, accept_rate=0.99, log
         torch.cuda.synchronize()
         t_cccs = ev_a.elapsed_time(ev_b)
         dmax = float(cccs.max())
-        engine.gamma_counts(net_dose, maker.grid.spacing, cccs, dose_norm=dmax, counts=judge_counts)
-        e, p = (int(v) for v in judge_counts[:2].cpu())
-        judge = p / e if e else 1.0
+        engine.gamma_counts(net_dose, maker.grid.spacing, cccs, dose_norm=dmax, counts=cccs_counts)
+        e, p = (int(v) for v in cccs_counts[:2].cpu())
+        vs_cccs = p / e if e else 1.0
         act = cccs > 0.1 * dmax
         mean_abs = float(((net_dose - cccs).abs()[act]).mean() / dmax) if bool(act.any()) else 0.0
         rows.append(dict(seed=int(s), gantry=float(cp.ga), accepted=bool(accepted), probe_pass=rate,
-                         n_probe=int(n_probe), judge_pass=judge, mean_abs_diff_frac=mean_abs, t_surrogate_ms=t_sur,
+                         n_probe=int(n_probe), gamma_vs_cccs=vs_cccs, mean_abs_diff_frac=mean_abs, t_surrogate_ms=t_sur,
                          t_cccs_ms=t_cccs))
         if log and (i + 1) % 25 == 0:
             acc = np.mean([r["accepted"] for r in rows])
-            log("eval %d/%d: accepted %.3f, judge mean %.4f" % (i + 1, len(seeds), acc,
-                                                               np.mean([r["judge_pass"] for r in rows])))
+            log("eval %d/%d: accepted %.3f, gamma vs CCCS mean %.4f" % (i + 1, len(seeds), acc,
+                                                               np.mean([r["gamma_vs_cccs"] for r in rows])))
     return rows
 
 
@@ -108,11 +108,11 @@ def summarize(rows, accept_rate):
     return dict(
         n=len(rows),
         accepted_frac=len(acc) / max(len(rows), 1),
-        judge_pass_mean_all=float(np.mean([r["judge_pass"] for r in rows])),
-        judge_pass_mean_accepted=float(np.mean([r["judge_pass"] for r in acc])) if acc else None,
-        judge_pass_min_accepted=float(np.min([r["judge_pass"] for r in acc])) if acc else None,
-        false_accepts=int(sum(1 for r in acc if r["judge_pass"] < accept_rate)),
-        beams_with_judge_ge_99=float(np.mean([r["judge_pass"] >= 0.99 for r in rows])),
+        gamma_vs_cccs_mean_all=float(np.mean([r["gamma_vs_cccs"] for r in rows])),
+        gamma_vs_cccs_mean_accepted=float(np.mean([r["gamma_vs_cccs"] for r in acc])) if acc else None,
+        gamma_vs_cccs_min_accepted=float(np.min([r["gamma_vs_cccs"] for r in acc])) if acc else None,
+        false_accepts=int(sum(1 for r in acc if r["gamma_vs_cccs"] < accept_rate)),
+        beams_gamma_vs_cccs_ge_99=float(np.mean([r["gamma_vs_cccs"] >= 0.99 for r in rows])),
         mean_abs_diff_frac=float(np.mean([r["mean_abs_diff_frac"] for r in rows])),
         ms_per_beam_surrogate_path=t_sur,
         ms_per_beam_cccs_path=t_cccs,

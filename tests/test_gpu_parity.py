@@ -3,7 +3,7 @@
   * the reference build itself at the full small-workload sizes
     (oracle/_ref, when present), and
   * the FP64 CPU oracle.
-Criteria (north star): |dD| <= 0.5 % of Dmax in every voxel above 10 % Dmax and
+Criteria: |dD| <= 0.5 % of Dmax in every voxel above 10 % Dmax and
 gamma(2 %/2 mm) >= 99.5 %; the engine is held to tighter bounds where the
 fixtures allow (noted per test)."""
 import glob

@@ -1,12 +1,12 @@
 """The trained photon surrogate with CCCS fallback (dosecuda_b200.surrogate).
 
 Held-out phantoms of the surrogate workload (seeds 1000000+i, never seen in
-training).  CCCS is the judge of every surrogate error: gamma(2%/2mm, 10%
+training).  CCCS is the arbiter of every surrogate error: gamma(2%/2mm, 10%
 cutoff, global maximum of the full CCCS dose).  Checked here:
 * a rejected (or forced) fallback returns exactly the full CCCS dose;
 * the trained network's dose is far closer to CCCS than the untrained
   network's (what training gains over the method without it);
-* a beam accepted by the probe passes the full-volume judge;
+* a beam accepted by the probe passes the full-volume gamma against CCCS;
 * masked voxels (TERMA <= 0.01) are exactly zero, as in CCCS."""
 import os
 
@@ -44,7 +44,7 @@ def _cccs(maker, density, cp):
     return maker.beam.dose()
 
 
-def _judge(engine, maker, dose, ref):
+def _gamma_vs_cccs(engine, maker, dose, ref):
     c = engine.gamma_counts(dose, maker.grid.spacing, ref, dose_norm=float(ref.max()))
     e, p = (int(v) for v in c[:2].cpu())
     return p / e
@@ -73,14 +73,14 @@ def test_training_gains_over_untrained_network(setup):
         for s, j, e in ((sur, jt, et), (sur_u, ju, eu)):
             _, acc, _, _ = s.dose(density, cp)
             d = s.pred.clone() if acc else s.pred * scale
-            j.append(_judge(engine, maker, d, ref))
+            j.append(_gamma_vs_cccs(engine, maker, d, ref))
             m = ref > 0.1 * ref.max()
             e.append(float((d - ref).abs()[m].mean() / ref.max()))
     assert np.mean(jt) > 0.95 and np.mean(jt) > np.mean(ju) + 0.5, (jt, ju)
     assert np.mean(et) < 0.25 * np.mean(eu), (et, eu)
 
 
-def test_accepted_beams_pass_the_judge_and_keep_the_mask(setup):
+def test_accepted_beams_pass_gamma_vs_cccs_and_keep_the_mask(setup):
     net, maker, sur, cases = setup
     from dosecuda_b200 import engine
     accepted_any = False
@@ -90,7 +90,7 @@ def test_accepted_beams_pass_the_judge_and_keep_the_mask(setup):
         if accepted:
             accepted_any = True
             assert rate >= 0.99
-            assert _judge(engine, maker, dose, ref) >= 0.98
+            assert _gamma_vs_cccs(engine, maker, dose, ref) >= 0.98
             assert torch.all(dose[sur.terma <= 0.01] == 0)
         else:
             assert torch.equal(dose, ref)
