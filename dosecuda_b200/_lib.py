@@ -104,6 +104,10 @@ SIGNATURES = {
                                       C.POINTER(C.c_longlong)]),
     "dc_proton_beam_dose": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "dc_proton_beam_adjoint": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "dc_proton_beam_dose_list": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p,
+                                           C.c_void_p]),
+    "dc_proton_beam_adjoint_list": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p,
+                                              C.c_void_p]),
     "dc_proton_beam_influence_nnz": (C.c_int, [C.c_void_p, C.c_void_p, C.c_float, C.POINTER(C.c_longlong),
                                                C.c_void_p]),
     "dc_proton_beam_influence_csr": (C.c_int, [C.c_void_p, C.c_void_p, C.c_float, C.c_void_p, C.c_void_p,

@@ -266,6 +266,45 @@ int dc_proton_beam_adjoint(dc_proton_beam *b, const float *wet_dev, const float 
     });
 }
 
+int dc_proton_beam_dose_list(dc_proton_beam *b, const float *wet_dev, const float *mu_dev, const int *voxels_dev,
+                             int n, float *out_dev, void *stream) {
+    return guarded([&] {
+        DeviceContext &ctx = beam_ctx(b);
+        need(wet_dev && voxels_dev && out_dev, "NULL device buffer.");
+        need(n >= 0, "'n' must not be negative.");
+        std::lock_guard<std::mutex> lk(ctx.mu);
+        cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+        ctx.begin_call(s);
+        PbExtra x;
+        x.mu = mu_dev;
+        x.list = voxels_dev;
+        x.n_list = n;
+        x.list_out = out_dev;
+        launch_pencil_beam_list(ctx, kPbDose, b->g, b->f, b->view(), wet_dev, x, s);
+        ctx.end_call(s);
+    });
+}
+
+int dc_proton_beam_adjoint_list(dc_proton_beam *b, const float *wet_dev, const int *voxels_dev, int n,
+                                const float *grad_dev, double *grad_mu_dev, void *stream) {
+    return guarded([&] {
+        DeviceContext &ctx = beam_ctx(b);
+        need(wet_dev && voxels_dev && grad_dev && grad_mu_dev, "NULL device buffer.");
+        need(n >= 0, "'n' must not be negative.");
+        std::lock_guard<std::mutex> lk(ctx.mu);
+        cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+        ctx.begin_call(s);
+        DC_CUDA(cudaMemsetAsync(grad_mu_dev, 0, (size_t)b->n_spots * sizeof(double), s));
+        PbExtra x;
+        x.grad_dose = grad_dev;
+        x.grad_mu = grad_mu_dev;
+        x.list = voxels_dev;
+        x.n_list = n;
+        launch_pencil_beam_list(ctx, kPbAdjoint, b->g, b->f, b->view(), wet_dev, x, s);
+        ctx.end_call(s);
+    });
+}
+
 int dc_proton_beam_influence_nnz(dc_proton_beam *b, const float *wet_dev, float cutoff, long long *nnz,
                                  void *stream) {
     return guarded([&] {

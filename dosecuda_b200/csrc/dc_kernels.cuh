@@ -63,6 +63,12 @@ struct PbExtra {
     int *col = nullptr;                // fill: spot index
     float *val = nullptr;              // fill: dose per MU
     long long cap = 0;                 // fill: capacity of col/val
+    // voxel-list mode (dose / adjoint only): the CTA's voxels are entries of
+    // `list` (flat voxel indices) instead of an image tile; `list_out` (dose)
+    // and grad_dose (adjoint) are then compact arrays indexed like `list`.
+    const int *list = nullptr;
+    int n_list = 0;
+    float *list_out = nullptr;
 };
 
 enum PbMode { kPbDose = 0, kPbAdjoint = 1, kPbSpotMax = 2, kPbCount = 3, kPbFill = 4 };
@@ -75,6 +81,10 @@ void build_proton_tables(const float *spots, int n_spots, const float *dvp, int 
 
 void launch_pencil_beam(DeviceContext &ctx, const Grid &g, const Frame &f, const ProtonTables &t,
                         const float *wet_s, float *dose, cudaStream_t s, const float *mu_dev = nullptr);
+// Dose (x.list_out) or adjoint (x.grad_dose compact, x.grad_mu) of the voxels
+// in x.list only; mode kPbDose or kPbAdjoint.
+void launch_pencil_beam_list(DeviceContext &ctx, int mode, const Grid &g, const Frame &f, const ProtonTables &t,
+                             const float *wet_s, const PbExtra &x, cudaStream_t s);
 
 // The other members of the family (see PbMode); `name` labels the profiler entry.
 void launch_pencil_beam_mode(DeviceContext &ctx, int mode, const Grid &g, const Frame &f, const ProtonTables &t,

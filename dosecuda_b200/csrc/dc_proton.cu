@@ -236,7 +236,9 @@ void launch_layer_rcut(const Grid &g, const Frame &f, LayerRec *layers, int n_la
 //   kPbSpotMax  spot_max[s]   = max_v K_s(v)
 //   kPbCount    counts[v]     = #{s : K_s(v) >= thr[s]}
 //   kPbFill     CSR row v     = (s, K_s(v)) for K_s(v) >= thr[s], in spot-table order
-template <int kMode, int TY, int VY>
+//   list mode   the CTA's voxels are x.list[bx*(threads*VY) + v*threads + tid]
+//               instead of an image tile (dose / adjoint of listed voxels)
+template <int kMode, int TY, int VY, bool kList = false>
 __device__ __forceinline__ void pb_tile(const Grid &g, const Frame &f, const ProtonTables &t,
                                         const float *__restrict__ wet_s, int bx, int by, int k, float (&acc)[VY],
                                         const PbExtra &x) {
@@ -267,12 +269,28 @@ __device__ __forceinline__ void pb_tile(const Grid &g, const Frame &f, const Pro
     bool inside[VY];
 #pragma unroll
     for (int v = 0; v < VY; ++v) {
-        const int j = j0 + v * TY;
-        inside[v] = (i < g.nx) && (j < g.ny);
+        int ic, jc, kc;
+        if constexpr (kList) {
+            const int e = bx * (kThreads * VY) + v * kThreads + tid;
+            const long long plane = (long long)g.nx * g.ny;
+            long long vi = x.list[min(e, x.n_list - 1)];
+            const bool valid = vi >= 0 && vi < plane * g.nz;  // out-of-grid entries give 0
+            inside[v] = e < x.n_list && valid;
+            vidx[v] = valid ? vi : 0;
+            kc = (int)(vidx[v] / plane);
+            const long long rem = vidx[v] - (long long)kc * plane;
+            jc = (int)(rem / g.nx);
+            ic = (int)(rem - (long long)jc * g.nx);
+        } else {
+            const int j = j0 + v * TY;
+            inside[v] = (i < g.nx) && (j < g.ny);
+            ic = min(i, g.nx - 1);
+            jc = min(j, g.ny - 1);
+            kc = k;
+            vidx[v] = (long long)ic + (long long)g.nx * (jc + (long long)g.ny * k);
+        }
         cnt[v] = 0;
-        const int ic = min(i, g.nx - 1), jc = min(j, g.ny - 1);
-        vidx[v] = (long long)ic + (long long)g.nx * (jc + (long long)g.ny * k);
-        const float3 p = voxel_xyz(g, f, ic, jc, k);
+        const float3 p = voxel_xyz(g, f, ic, jc, kc);
         const float3 h = image_to_head<false>(f, p);
         hx[v] = h.x;
         hy[v] = h.y;
@@ -281,7 +299,12 @@ __device__ __forceinline__ void pb_tile(const Grid &g, const Frame &f, const Pro
         dsrc[v] = distance_to_source(f, p);
         wet_mm[v] = __ldg(wet_s + vidx[v]) * 10.0f;
         gv[v] = 0.0f;
-        if (kMode == kPbAdjoint) gv[v] = inside[v] ? __ldg(x.grad_dose + vidx[v]) : 0.0f;
+        if (kMode == kPbAdjoint) {
+            if constexpr (kList)
+                gv[v] = inside[v] ? __ldg(x.grad_dose + bx * (kThreads * VY) + v * kThreads + tid) : 0.0f;
+            else
+                gv[v] = inside[v] ? __ldg(x.grad_dose + vidx[v]) : 0.0f;
+        }
         fill_off[v] = fill_end[v] = 0;
         if (kMode == kPbFill && inside[v]) {
             fill_off[v] = x.row_ptr[vidx[v]];
@@ -598,6 +621,26 @@ __global__ void __launch_bounds__(kPbThreadsX *TY, pb_min_ctas(TY, 4))
     }
 }
 
+// Voxel-list kernel (dose / adjoint of listed voxels; one CTA per
+// threads*VY consecutive list entries).  A sorted list keeps a CTA's voxels
+// close together, so the per-CTA spot culling stays tight.
+template <int kMode, int TY, int VY>
+__global__ void __launch_bounds__(kPbThreadsX *TY, pb_min_ctas(TY, 4))
+    pb_list_kernel(Grid g, Frame f, ProtonTables t, const float *__restrict__ wet_s, PbExtra x) {
+    float acc[VY];
+#pragma unroll
+    for (int v = 0; v < VY; ++v) acc[v] = 0.0f;
+    pb_tile<kMode, TY, VY, true>(g, f, t, wet_s, blockIdx.x, 0, 0, acc, x);
+    if (kMode == kPbDose) {
+        const int tid = threadIdx.y * kPbThreadsX + threadIdx.x;
+#pragma unroll
+        for (int v = 0; v < VY; ++v) {
+            const int e = blockIdx.x * (kPbThreadsX * TY * VY) + v * (kPbThreadsX * TY) + tid;
+            if (e < x.n_list) x.list_out[e] = acc[v];
+        }
+    }
+}
+
 // Persistent batch kernel: CTAs take (plan, tile) work items from a device
 // queue (most expensive plans first) and sum the dose of all the plan's beams
 // for the tile in registers before one write per voxel.
@@ -678,6 +721,30 @@ void launch_pencil_beam_mode(DeviceContext &ctx, int mode, const Grid &g, const 
         case kPbCount: pb_launch<kPbCount>(ctx, "pencil_beam_count", g, f, t, wet_s, nullptr, x, s); break;
         case kPbFill: pb_launch<kPbFill>(ctx, "pencil_beam_fill", g, f, t, wet_s, nullptr, x, s); break;
         default: throw Error(DC_ERR_VALUE, "unknown pencil-beam mode");
+    }
+}
+
+template <int kMode>
+static void pb_list_launch(DeviceContext &ctx, const char *name, const Grid &g, const Frame &f,
+                           const ProtonTables &t, const float *wet_s, const PbExtra &x, cudaStream_t s) {
+    if (x.n_list <= 0) return;
+    const size_t smem = pb_smem(t.lut_len);
+    static bool attr_set[64] = {false};
+    pb_attr(pb_list_kernel<kMode, kPbThreadsY, kPbVoxY>, smem, ctx.device, attr_set);
+    const int per_cta = kPbThreadsX * kPbThreadsY * kPbVoxY;
+    const unsigned blocks = (unsigned)((x.n_list + per_cta - 1) / per_cta);
+    KernelTimer kt(ctx, name, s);
+    pb_list_kernel<kMode, kPbThreadsY, kPbVoxY><<<blocks, dim3(kPbThreadsX, kPbThreadsY, 1), smem, s>>>(g, f, t,
+                                                                                                     wet_s, x);
+    check_launch(name);
+}
+
+void launch_pencil_beam_list(DeviceContext &ctx, int mode, const Grid &g, const Frame &f, const ProtonTables &t,
+                             const float *wet_s, const PbExtra &x, cudaStream_t s) {
+    switch (mode) {
+        case kPbDose: pb_list_launch<kPbDose>(ctx, "pencil_beam_list", g, f, t, wet_s, x, s); break;
+        case kPbAdjoint: pb_list_launch<kPbAdjoint>(ctx, "pencil_beam_list_adjoint", g, f, t, wet_s, x, s); break;
+        default: throw Error(DC_ERR_VALUE, "voxel-list mode is for the dose and the adjoint");
     }
 }
 

@@ -209,6 +209,48 @@ class ProtonBeamPlan:
         _lib.raise_for(rc)
         return out
 
+    @staticmethod
+    def _voxels(voxels: torch.Tensor, device) -> torch.Tensor:
+        v = voxels.to(device=device, dtype=torch.int32).reshape(-1).contiguous()
+        if v.numel() >= 2 ** 31:
+            raise ValueError("voxel lists are limited to 2^31 - 1 entries")
+        return v
+
+    def dose_list(self, wet: torch.Tensor, voxels: torch.Tensor, mu: torch.Tensor | None = None,
+                  stream=None) -> torch.Tensor:
+        """Dose (float32) at the listed voxels only (flat indices into the
+        grid, best sorted); entries outside the grid give 0."""
+        _check_volume(wet, "wet")
+        h = self._handle(tuple(wet.shape))
+        vox = self._voxels(voxels, wet.device)
+        out = torch.empty(vox.numel(), dtype=torch.float32, device=wet.device)
+        mu_p = None
+        if mu is not None:
+            mu = mu.detach().to(device=wet.device, dtype=torch.float32).contiguous()
+            if mu.numel() != self.n_spots:
+                raise ValueError("mu must hold one weight per spot")
+            mu_p = C.c_void_p(mu.data_ptr())
+        _lib.raise_for(_lib.load().dc_proton_beam_dose_list(h, C.c_void_p(wet.data_ptr()), mu_p,
+                                                            C.c_void_p(vox.data_ptr()), vox.numel(),
+                                                            C.c_void_p(out.data_ptr()), _stream(wet, stream)))
+        return out
+
+    def adjoint_list(self, wet: torch.Tensor, voxels: torch.Tensor, grad: torch.Tensor, stream=None) -> torch.Tensor:
+        """D^T g for a gradient given at the listed voxels only (float64,
+        one entry per spot)."""
+        _check_volume(wet, "wet")
+        h = self._handle(tuple(wet.shape))
+        vox = self._voxels(voxels, wet.device)
+        g = grad.detach().to(device=wet.device, dtype=torch.float32).reshape(-1).contiguous()
+        if g.numel() != vox.numel():
+            raise ValueError("one gradient value per listed voxel is required")
+        out = torch.empty(self.n_spots, dtype=torch.float64, device=wet.device)
+        _lib.raise_for(_lib.load().dc_proton_beam_adjoint_list(h, C.c_void_p(wet.data_ptr()),
+                                                               C.c_void_p(vox.data_ptr()), vox.numel(),
+                                                               C.c_void_p(g.data_ptr()), C.c_void_p(out.data_ptr()),
+                                                               _stream(wet, stream)))
+        return out
+
     def influence_csr(self, wet: torch.Tensor, cutoff: float = 1e-4, stream=None):
         """(row_ptr int64[n_voxels+1], col int32[nnz], val float32[nnz]) of the
         voxels x spots influence matrix, entries >= cutoff x the spot's maximum."""
@@ -241,6 +283,27 @@ class _ProtonDoseFn(torch.autograd.Function):
         (wet,) = ctx.saved_tensors
         g = ctx.plan.adjoint(wet, grad_dose)
         return g.to(ctx.mu_dtype), None, None
+
+
+class _ProtonDoseListFn(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, mu, wet, plan, voxels):
+        ctx.plan, ctx.voxels = plan, voxels
+        ctx.save_for_backward(wet)
+        ctx.mu_dtype = mu.dtype
+        return plan.dose_list(wet, voxels, mu)
+
+    @staticmethod
+    def backward(ctx, grad):
+        (wet,) = ctx.saved_tensors
+        return ctx.plan.adjoint_list(wet, ctx.voxels, grad).to(ctx.mu_dtype), None, None, None
+
+
+def proton_dose_list_autograd(mu: torch.Tensor, wet: torch.Tensor, plan: "ProtonBeamPlan",
+                              voxels: torch.Tensor) -> torch.Tensor:
+    """Differentiable dose of one beam at the listed voxels only (the voxel-
+    list forms of the pencil-beam kernel and of its adjoint)."""
+    return _ProtonDoseListFn.apply(mu, wet, plan, voxels)
 
 
 def proton_dose_autograd(mu: torch.Tensor, wet: torch.Tensor, plan: ProtonBeamPlan) -> torch.Tensor:

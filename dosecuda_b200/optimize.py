@@ -14,6 +14,10 @@ behind ``torch.autograd`` (``engine.proton_dose_autograd``).
 * ``ImptOptimizer``: projected Adam on the spot weights (weights >= 0 after
   every step); ``save``/``load`` write and restore the weights, Adam's moments
   and step count and the iteration, so an interrupted run continues exactly.
+  With ``voxels="objective"`` every step computes the dose and the adjoint
+  at the objective's voxels only (``ProtonBeamPlan.dose_list`` /
+  ``adjoint_list``): the objective and its gradient depend on nothing else,
+  and target plus organs at risk are a small part of the grid.
 * ``save_influence_csr``/``load_influence_csr``: a dose-influence matrix
   (``ProtonBeamPlan.influence_csr``) cached as ``.npz``."""
 from __future__ import annotations
@@ -35,6 +39,8 @@ class DoseObjective:
 
     def __init__(self):
         self.terms = []
+        self._union = None
+        self._pos = None
 
     @staticmethod
     def _index(mask: torch.Tensor) -> torch.Tensor:
@@ -58,6 +64,30 @@ class DoseObjective:
 
     def min_dose(self, mask, dose, weight=1.0):
         return self.add("min", mask, dose, weight)
+
+    def voxel_union(self) -> torch.Tensor:
+        """Sorted flat indices of every voxel some term reads (the only
+        voxels whose dose the objective depends on)."""
+        if self._pos is None or len(self._pos) != len(self.terms):
+            if not self.terms:
+                raise ValueError("the objective has no terms")
+            self._union = torch.unique(torch.cat([t[1] for t in self.terms]))
+            self._pos = [torch.searchsorted(self._union, t[1]) for t in self.terms]
+        return self._union
+
+    def on_list(self, dose_list: torch.Tensor) -> torch.Tensor:
+        """The objective from the dose at voxel_union() only (same terms,
+        same float64 arithmetic as __call__)."""
+        self.voxel_union()
+        f = torch.zeros((), dtype=torch.float64, device=dose_list.device)
+        for (kind, _, d, w, _), pos in zip(self.terms, self._pos):
+            r = dose_list.index_select(0, pos).double() - d
+            if kind == "max":
+                r = torch.clamp(r, min=0.0)
+            elif kind == "min":
+                r = torch.clamp(r, max=0.0)
+            f = f + w * (r * r).sum()
+        return f
 
     def __call__(self, dose: torch.Tensor) -> torch.Tensor:
         flat = dose.reshape(-1)
@@ -83,7 +113,7 @@ class ImptOptimizer:
     order; ``lr`` defaults to ``lr_frac`` x the mean initial weight."""
 
     def __init__(self, plans, wets, objective: DoseObjective, mu: torch.Tensor | None = None, lr: float | None = None,
-                 lr_frac: float = 0.02):
+                 lr_frac: float = 0.02, voxels: str = "volume"):
         self.plans, self.wets = list(plans), list(wets)
         if len(self.plans) != len(self.wets) or not self.plans:
             raise ValueError("one WET volume per beam is required")
@@ -97,6 +127,13 @@ class ImptOptimizer:
         self.opt = torch.optim.Adam([self.mu], lr=self.lr)
         self.iteration = 0
         self.value = None  # objective (device tensor) at the weights before the last step
+        if voxels not in ("volume", "objective"):
+            raise ValueError("voxels must be 'volume' or 'objective'")
+        # "objective": each step evaluates the dose and its adjoint at the
+        # objective's voxels only (the voxel-list kernels), which gives the
+        # same objective and gradient for a fraction of the work
+        self.voxels = voxels
+        self._list = objective.voxel_union().to(torch.int32) if voxels == "objective" else None
 
     def dose(self, mu: torch.Tensor | None = None) -> torch.Tensor:
         """Total dose of all beams; differentiable in ``mu`` (default: the
@@ -109,9 +146,26 @@ class ImptOptimizer:
             total = d if total is None else total + d
         return total
 
+    def dose_list(self, mu: torch.Tensor | None = None) -> torch.Tensor:
+        """Total dose at the objective's voxels (``objective.voxel_union()``);
+        differentiable in ``mu``."""
+        m = self.mu if mu is None else mu
+        vox = self._list if self._list is not None else self.objective.voxel_union().to(torch.int32)
+        parts = torch.split(m, self.sizes)
+        total = None
+        for q, w, p in zip(parts, self.wets, self.plans):
+            d = engine.proton_dose_list_autograd(q.contiguous(), w, p, vox)
+            total = d if total is None else total + d
+        return total
+
+    def _objective(self, mu: torch.Tensor) -> torch.Tensor:
+        if self.voxels == "objective":
+            return self.objective.on_list(self.dose_list(mu))
+        return self.objective(self.dose(mu))
+
     def evaluate(self) -> float:
         with torch.no_grad():
-            return float(self.objective(self.dose(self.mu.detach())))
+            return float(self._objective(self.mu.detach()))
 
     def scale_to(self, mask: torch.Tensor, dose: float) -> float:
         """Scales the weights so that the mean dose over ``mask`` is ``dose``
@@ -134,7 +188,7 @@ class ImptOptimizer:
         """One iteration: dose, objective, adjoint gradient, Adam, projection
         onto mu >= 0.  Does not synchronise with the host."""
         self.opt.zero_grad(set_to_none=True)
-        f = self.objective(self.dose())
+        f = self._objective(self.mu)
         f.backward()
         self.opt.step()
         with torch.no_grad():

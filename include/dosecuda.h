@@ -258,6 +258,17 @@ int dc_proton_beam_dose(dc_proton_beam *beam, const float *wet_dev, const float 
 /* grad_mu_dev[s] = sum_v grad_dose_dev[v] K_s(v) (FP64, overwritten). */
 int dc_proton_beam_adjoint(dc_proton_beam *beam, const float *wet_dev, const float *grad_dose_dev,
                            double *grad_mu_dev, void *stream);
+/* Voxel-list forms (no reference counterpart): the dose of the n voxels
+ * listed in voxels_dev (flat indices into the beam's grid; entries outside
+ * the grid give 0) into out_dev[0..n), and the adjoint of a gradient given
+ * at those voxels only (grad_dev[0..n)) into grad_mu_dev (n_spots doubles,
+ * overwritten).  The same per-pair influence as the volume forms; an
+ * objective defined on a voxel subset (target, organs at risk) needs only
+ * these.  A list sorted by voxel index keeps each CTA's voxels together. */
+int dc_proton_beam_dose_list(dc_proton_beam *b, const float *wet_dev, const float *mu_dev, const int *voxels_dev,
+                             int n, float *out_dev, void *stream);
+int dc_proton_beam_adjoint_list(dc_proton_beam *b, const float *wet_dev, const int *voxels_dev, int n,
+                                const float *grad_dev, double *grad_mu_dev, void *stream);
 
 /* Influence matrix A (voxels x spots) in CSR with voxel rows: entries
  * K_s(v) >= cutoff * max_v K_s(v).  _nnz computes the entry count

@@ -83,3 +83,47 @@ def test_influence_cache_reproduces_the_dose(setup, tmp_path):
     ref = bp.dose(wets[0]).reshape(-1).double()
     torch.cuda.synchronize()
     assert (d - ref).abs().max().item() <= 1e-5 * ref.max().item()
+
+
+def test_voxel_list_dose_and_adjoint_equal_the_volume_forms(setup):
+    torch, engine, grid, model, beams, wets, target, oar = setup
+    bp = engine.ProtonBeamPlan(grid, beams[0], model)
+    wet = wets[0]
+    vox = torch.nonzero((target | oar).reshape(-1)).squeeze(1)
+    full = bp.dose(wet).reshape(-1)
+    lst = bp.dose_list(wet, vox)
+    ref = full[vox]
+    scale = float(ref.abs().max())
+    assert scale > 0 and float((lst - ref).abs().max()) <= 1e-6 * scale
+    # entries outside the grid give 0, the others are unaffected
+    bad = torch.tensor([-1, wet.numel(), int(vox[0])], device="cuda")
+    out = bp.dose_list(wet, bad)
+    assert float(out[0]) == 0.0 and float(out[1]) == 0.0 and float(out[2]) == float(lst[0])
+    g = torch.randn(vox.numel(), device="cuda", generator=torch.Generator("cuda").manual_seed(5))
+    g_full = torch.zeros(wet.numel(), device="cuda")
+    g_full[vox] = g
+    a_full = bp.adjoint(wet, g_full.reshape(wet.shape))
+    a_list = bp.adjoint_list(wet, vox, g)
+    torch.cuda.synchronize()
+    assert float((a_list - a_full).abs().max()) <= 1e-5 * float(a_full.abs().max())
+
+
+def test_objective_voxel_optimiser_follows_the_volume_one(setup):
+    torch = setup[0]
+    from dosecuda_b200.optimize import ImptOptimizer
+    vol = _optimizer(setup)
+    f0 = vol.evaluate()
+    vol.run(30)
+    obj = vol.objective
+    lst = ImptOptimizer(vol.plans, vol.wets, obj, voxels="objective")
+    lst.scale_to(setup[6], 2.0)
+    assert abs(lst.evaluate() - f0) <= 1e-5 * f0
+    lst.run(30)
+    torch.cuda.synchronize()
+    with torch.no_grad():
+        f_vol = float(obj(vol.dose()))
+        f_lst = float(obj(lst.dose()))
+    assert f_lst < 0.5 * f0
+    assert abs(f_lst - f_vol) <= 1e-3 * f0
+    a, b = vol.mu.detach().double(), lst.mu.detach().double()
+    assert float((a - b).abs().max()) <= 1e-3 * float(a.abs().max())
