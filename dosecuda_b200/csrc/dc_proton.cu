@@ -389,6 +389,10 @@ __device__ __forceinline__ void pb_tile(const Grid &g, const Frame &f, const Pro
 #pragma unroll
         for (int v = 0; v < VY; ++v) {
             act[v] = inside[v] && pb_voxel_layer(L, s_depth, s_sigma, s_idd, t.lut_len, wet_mm[v], dsrc[v], pv[v]);
+            // adjoint: a voxel with zero gradient adds exactly zero to every
+            // spot's sum, so it counts as inactive (an objective's gradient
+            // vanishes outside its voxel sets)
+            if (kMode == kPbAdjoint) act[v] = act[v] && gv[v] != 0.0f;
             if (!act[v]) {
                 pv[v].pf = pv[v].hf = 0.f;
                 pv[v].ps2 = pv[v].hs2 = 0.f;
@@ -514,8 +518,11 @@ __device__ __forceinline__ void pb_tile(const Grid &g, const Frame &f, const Pro
                     if (act[v]) acc[v] += fmaf(pv[v].pf, accp[v], pv[v].hf * acch[v]);
                 }
             } else {
-                // modes that need the per-pair influence K_s(v)
-                for (int q = 0; q < cn; ++q) {
+                // modes that need the per-pair influence K_s(v); a warp
+                // without an active voxel contributes nothing and skips the
+                // spots as a whole (its shuffles stay warp-uniform)
+                const bool warp_any = __any_sync(0xffffffffu, any);
+                for (int q = 0; q < (warp_any ? cn : 0); ++q) {
                     const float4 a = s_spot_a[q];
                     const float4 b = s_spot_b[q];
                     float kv[VY];
