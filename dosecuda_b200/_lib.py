@@ -158,6 +158,7 @@ SIGNATURES = {
     "dc_net_tc_error": (C.c_int, [C.c_int, C.POINTER(C.c_int)]),
     "dc_net_tc_selftest": (C.c_int, [C.c_int, C.POINTER(C.c_int)]),
     "dc_host_buffer_mapped": (C.c_int, [C.c_int, C.c_void_p, C.c_ulonglong, C.POINTER(C.c_int)]),
+    "dc_debug_bounds": (C.c_int, [C.c_int, C.POINTER(C.c_ulonglong), C.POINTER(C.c_int)]),
     "dc_basis_combine_dev": (C.c_int, [C.c_int, C.c_void_p, C.c_int, C.c_longlong, C.c_void_p, C.c_void_p,
                                        C.c_void_p]),
     "dc_basis_adjoint_dev": (C.c_int, [C.c_int, C.c_void_p, C.c_int, C.c_longlong, C.c_void_p, C.c_void_p,

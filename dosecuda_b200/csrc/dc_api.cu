@@ -108,6 +108,25 @@ extern "C" {
 
 const char *dc_last_error(void) { return dc::last_error_cstr(); }
 
+int dc_debug_bounds(int gpu_id, unsigned long long *violation, int *enabled) {
+    return guarded([&] {
+        need(violation != nullptr && enabled != nullptr, "output pointers must not be NULL.");
+#ifdef DC_DEBUG_BOUNDS
+        *enabled = 1;
+#else
+        *enabled = 0;
+#endif
+        DeviceContext &ctx = context(gpu_id);
+        std::lock_guard<std::mutex> lk(ctx.mu);
+        DC_CUDA(cudaDeviceSynchronize());
+        unsigned long long v = 0;
+        for (unsigned long long w : {take_bounds_wet(), take_bounds_photon(), take_bounds_proton(),
+                                     take_bounds_basis()})
+            if (v == 0) v = w;
+        *violation = v;
+    });
+}
+
 int dc_host_buffer_mapped(int gpu_id, const void *host, unsigned long long bytes, int *mapped) {
     return guarded([&] {
         need(mapped != nullptr, "'mapped' must not be NULL.");

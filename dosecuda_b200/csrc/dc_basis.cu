@@ -21,9 +21,13 @@
 #include <algorithm>
 
 #include "../../include/dosecuda.h"
+#include "dc_common.cuh"
 #include "dc_runtime.cuh"
 
 namespace dc {
+
+DC_BOUNDS_WORD
+
 namespace {
 
 constexpr int kBasisThreads = 256;
@@ -39,9 +43,13 @@ __global__ void __launch_bounds__(kBasisThreads) basis_combine_kernel(const floa
                                                                       float *__restrict__ out) {
     for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < n; v += (long long)gridDim.x * blockDim.x) {
         float acc = out[v];
-        for (int b = 0; b < n_basis; ++b)
-            acc = __double2float_rn(__dadd_rn((double)acc, __dmul_rn((double)__ldg(basis + (long long)b * n + v),
+        for (int b = 0; b < n_basis; ++b) {
+            const long long u = (long long)b * n + v;
+            acc = __double2float_rn(__dadd_rn((double)acc, __dmul_rn(DC_IN_BOUNDS(u, (long long)n_basis * n, 30)
+                                                                          ? (double)__ldg(basis + u)
+                                                                          : 0.0,
                                                                       __ldg(coef + b))));
+        }
         out[v] = acc;
     }
 }
@@ -75,6 +83,9 @@ void check_basis(const float *basis, int n_basis, long long n_vox) {
 }
 
 }  // namespace
+
+DC_BOUNDS_TAKE(take_bounds_basis)
+
 }  // namespace dc
 
 extern "C" {

@@ -22,6 +22,37 @@
 #include <math_constants.h>
 #include <stdint.h>
 
+// Debug builds (-DDC_DEBUG_BOUNDS; `python -m dosecuda_b200.build
+// --debug-bounds --out PATH`) check the index of each instrumented global
+// access against its buffer's extent.  The first violation in a translation
+// unit is recorded in that unit's error word (site << 48 | index & 2^48-1)
+// and the access is skipped, so an indexing bug shows up as a report
+// (dc_debug_bounds) instead of a fault.  Release builds compile the checks
+// away: DC_IN_BOUNDS is the constant true.
+#ifdef DC_DEBUG_BOUNDS
+#define DC_BOUNDS_WORD static __device__ unsigned long long g_dc_bounds = 0ull;
+__device__ __forceinline__ bool dc_in_bounds_impl(unsigned long long *word, long long idx, long long n,
+                                                  unsigned site) {
+    if (idx >= 0 && idx < n) return true;
+    atomicCAS(word, 0ull, ((unsigned long long)site << 48) | ((unsigned long long)idx & 0xFFFFFFFFFFFFull));
+    return false;
+}
+#define DC_IN_BOUNDS(idx, n, site) \
+    ::dc_in_bounds_impl(&g_dc_bounds, (long long)(idx), (long long)(n), (unsigned)(site))
+#define DC_BOUNDS_TAKE(fn)                                                          \
+    unsigned long long fn() {                                                       \
+        unsigned long long v = 0ull, z = 0ull;                                      \
+        if (cudaMemcpyFromSymbol(&v, g_dc_bounds, sizeof(v)) != cudaSuccess) v = ~0ull; \
+        cudaMemcpyToSymbol(g_dc_bounds, &z, sizeof(z));                             \
+        return v;                                                                   \
+    }
+#else
+#define DC_BOUNDS_WORD
+#define DC_IN_BOUNDS(idx, n, site) true
+#define DC_BOUNDS_TAKE(fn) \
+    unsigned long long fn() { return 0ull; }
+#endif
+
 namespace dc {
 
 constexpr float kAirDensity = 0.0012f;  // g/cc, IMRTClasses.cuh:6

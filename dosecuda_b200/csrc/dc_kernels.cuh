@@ -73,6 +73,13 @@ struct PbExtra {
 
 enum PbMode { kPbDose = 0, kPbAdjoint = 1, kPbSpotMax = 2, kPbCount = 3, kPbFill = 4 };
 
+// First bounds violation recorded by each translation unit's checked
+// accesses since the last call, and cleared (debug builds; 0 otherwise).
+unsigned long long take_bounds_wet();
+unsigned long long take_bounds_photon();
+unsigned long long take_bounds_proton();
+unsigned long long take_bounds_basis();
+
 // Builds the sorted spot table and the layer table on the host.  Throws
 // Error(DC_ERR_VALUE) for malformed input.
 void build_proton_tables(const float *spots, int n_spots, const float *dvp, int n_energies, int dvp_len,

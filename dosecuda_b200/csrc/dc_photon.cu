@@ -48,6 +48,8 @@
 
 namespace dc {
 
+DC_BOUNDS_WORD
+
 // ---------------------------------------------------------------------------
 // TERMA
 // ---------------------------------------------------------------------------
@@ -182,11 +184,12 @@ __global__ void __launch_bounds__(128) terma_kernel(Grid g, Frame f, PhotonParam
     const float T = oaf * ((1.0f - P.ssw) * tp * terma + P.ssw * ts * terma);
     const float rho = tex3D<float>(dens_tex, (float)i + 0.5f, (float)j + 0.5f, (float)k + 0.5f);
     surf3Dwrite(make_float2(T, rho), td_surf, i * (int)sizeof(float2), j, k);
-    electron[v] = P.esw * (0.4f + (0.3f * ratio)) * elec * tp;
-    if (terma_out) terma_out[v] = T;
+    const bool v_ok = DC_IN_BOUNDS(v, g.n(), 10);
+    if (v_ok) electron[v] = P.esw * (0.4f + (0.3f * ratio)) * elec * tp;
+    if (terma_out && v_ok) terma_out[v] = T;
 
     const bool act = !(T <= 0.01f);
-    if (!act && dose) dose[v] = 0.0f;
+    if (!act && dose && v_ok) dose[v] = 0.0f;
     const unsigned live = __activemask();
     const unsigned bal = __ballot_sync(live, act);
     if (act) {
@@ -195,7 +198,8 @@ __global__ void __launch_bounds__(128) terma_kernel(Grid g, Frame f, PhotonParam
         unsigned base = 0;
         if (lane == leader) base = atomicAdd(n_active, (unsigned)__popc(bal));
         base = __shfl_sync(bal, base, leader);
-        active[base + __popc(bal & ((1u << lane) - 1u))] = (int)v;
+        const long long slot = (long long)base + __popc(bal & ((1u << lane) - 1u));
+        if (DC_IN_BOUNDS(slot, g.n(), 12)) active[slot] = (int)v;
     }
 }
 
@@ -243,7 +247,8 @@ __global__ void __launch_bounds__(128) cccs_kernel(Grid g, Frame f, CccsCones C,
     const unsigned n = *n_active;
     const int plane = g.nx * g.ny;
     for (unsigned t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
-        const int v = __ldg(active + t);
+        const int v = DC_IN_BOUNDS(t, g.n(), 13) ? __ldg(active + t) : -1;
+        if (!DC_IN_BOUNDS(v, g.n(), 13)) continue;
         const int k = v / plane;
         const int rem = v - k * plane;
         const int j = rem / g.nx;
@@ -251,7 +256,7 @@ __global__ void __launch_bounds__(128) cccs_kernel(Grid g, Frame f, CccsCones C,
         const float3 p = voxel_xyz(g, f, i, j, k);
         float dose_value = cccs_voxel(g, f, C, sp_cm, s_dir, s_rl10, td_tex, p);
         dose_value += __ldg(electron + v);
-        dose[v] = (!isnan(dose_value) && dose_value >= 0.0f) ? dose_scale * dose_value : 0.0f;
+        dose[v] = (!isnan(dose_value) && dose_value >= 0.0f) ? dose_scale * dose_value : 0.0f;  // v checked above
     }
 }
 
@@ -446,6 +451,8 @@ static unsigned cccs_blocks(const DeviceContext &ctx, long long work) {
     const long long want = (work + 127) / 128;
     return (unsigned)std::max(1LL, std::min<long long>(want, (long long)sms * std::max(per_sm, 1)));
 }
+
+DC_BOUNDS_TAKE(take_bounds_photon)
 
 void enqueue_terma(DeviceContext &ctx, const Grid &g, const Frame &f, const PhotonParams &P, const CccsCones &C,
                    const PhotonWork &w, float *dose_dev, float *terma_out, cudaStream_t s) {

@@ -38,6 +38,8 @@
 
 namespace dc {
 
+DC_BOUNDS_WORD
+
 constexpr int kPbThreadsX = 32;
 constexpr int kPbThreadsY = 8;
 constexpr int kPbVoxY = 2;      // voxels per thread along y
@@ -297,7 +299,7 @@ __device__ __forceinline__ void pb_tile(const Grid &g, const Frame &f, const Pro
         hz[v] = h.z;
         hz2[v] = h.z * h.z;
         dsrc[v] = distance_to_source(f, p);
-        wet_mm[v] = __ldg(wet_s + vidx[v]) * 10.0f;
+        wet_mm[v] = (DC_IN_BOUNDS(vidx[v], g.n(), 21) ? __ldg(wet_s + vidx[v]) : 0.0f) * 10.0f;
         gv[v] = 0.0f;
         if (kMode == kPbAdjoint) {
             if constexpr (kList)
@@ -596,7 +598,7 @@ __device__ __forceinline__ void pb_tile(const Grid &g, const Frame &f, const Pro
     if (kMode == kPbCount) {
 #pragma unroll
         for (int v = 0; v < VY; ++v)
-            if (inside[v]) x.counts[vidx[v]] = cnt[v];
+            if (inside[v] && DC_IN_BOUNDS(vidx[v], g.n(), 24)) x.counts[vidx[v]] = cnt[v];
     }
 }
 
@@ -623,7 +625,8 @@ __global__ void __launch_bounds__(kPbThreadsX *TY, pb_min_ctas(TY, 4))
 #pragma unroll
         for (int v = 0; v < VY; ++v) {
             const int j = blockIdx.y * (TY * VY) + threadIdx.y + v * TY;
-            if (i < g.nx && j < g.ny) dose[(long long)i + (long long)g.nx * (j + (long long)g.ny * blockIdx.z)] = acc[v];
+            const long long u = (long long)i + (long long)g.nx * (j + (long long)g.ny * blockIdx.z);
+            if (i < g.nx && j < g.ny && DC_IN_BOUNDS(u, g.n(), 20)) dose[u] = acc[v];
         }
     }
 }
@@ -643,7 +646,7 @@ __global__ void __launch_bounds__(kPbThreadsX *TY, pb_min_ctas(TY, 4))
 #pragma unroll
         for (int v = 0; v < VY; ++v) {
             const int e = blockIdx.x * (kPbThreadsX * TY * VY) + v * (kPbThreadsX * TY) + tid;
-            if (e < x.n_list) x.list_out[e] = acc[v];
+            if (e < x.n_list && DC_IN_BOUNDS(e, x.n_list, 22)) x.list_out[e] = acc[v];
         }
     }
 }
@@ -682,10 +685,13 @@ __global__ void __launch_bounds__(kPbThreadsX *TY, pb_min_ctas(TY, 3))
 #pragma unroll
         for (int v = 0; v < VY; ++v) {
             const int j = by * (TY * VY) + threadIdx.y + v * TY;
-            if (i < P.g.nx && j < P.g.ny) P.dose[(long long)i + (long long)P.g.nx * (j + (long long)P.g.ny * k)] = acc[v];
+            const long long u = (long long)i + (long long)P.g.nx * (j + (long long)P.g.ny * k);
+            if (i < P.g.nx && j < P.g.ny && DC_IN_BOUNDS(u, P.g.n(), 23)) P.dose[u] = acc[v];
         }
     }
 }
+
+DC_BOUNDS_TAKE(take_bounds_proton)
 
 static size_t pb_smem(int lut_len) {
     return 2 * kPbSpotChunk * sizeof(float4) + kPbSpotChunk * sizeof(float) + 3 * (size_t)lut_len * sizeof(float);

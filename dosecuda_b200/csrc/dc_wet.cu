@@ -23,6 +23,8 @@
 
 namespace dc {
 
+DC_BOUNDS_WORD
+
 __global__ void __launch_bounds__(128) wet_march_kernel(Grid g, Frame f, cudaTextureObject_t density,
                                                         float *__restrict__ wet) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -48,7 +50,8 @@ __global__ void __launch_bounds__(128) wet_march_kernel(Grid g, Frame f, cudaTex
         wet_sum = fmaf(fmaxf(rho, 0.0f), 0.1f, wet_sum);
         t += 1.0f;
     }
-    wet[(long long)i + (long long)g.nx * (j + (long long)g.ny * k)] = wet_sum;
+    const long long v = (long long)i + (long long)g.nx * (j + (long long)g.ny * k);
+    if (DC_IN_BOUNDS(v, g.n(), 1)) wet[v] = wet_sum;
 }
 
 // Nearest voxel index (int)roundf(v / s) of the reference's smoothing
@@ -89,7 +92,7 @@ __global__ void __launch_bounds__(128) wet_smooth_kernel(Grid g, Frame f, const 
     const long long v = (long long)i + (long long)g.nx * (j + (long long)g.ny * k);
     const float3 p = voxel_xyz(g, f, i, j, k);
     const float3 h = image_to_head<false>(f, p);
-    const float c = __ldg(wet + v);
+    const float c = DC_IN_BOUNDS(v, g.n(), 2) ? __ldg(wet + v) : 0.0f;
     const float rmax = c * 10.0f;
     const float rsx = 1.0f / g.sx, rsy = 1.0f / g.sy, rsz = 1.0f / g.sz;
     float sum = c;
@@ -105,17 +108,20 @@ __global__ void __launch_bounds__(128) wet_smooth_kernel(Grid g, Frame f, const 
             const int qk = nearest_index(q.z + f.isoz, g.sz, rsz);
             if ((unsigned)qi < (unsigned)g.nx && (unsigned)qj < (unsigned)g.ny &&
                 (unsigned)qk < (unsigned)g.nz) {
-                sum += __ldg(wet + (long long)qi + (long long)g.nx * (qj + (long long)g.ny * qk));
+                const long long u = (long long)qi + (long long)g.nx * (qj + (long long)g.ny * qk);
+                sum += DC_IN_BOUNDS(u, g.n(), 3) ? __ldg(wet + u) : 0.0f;
                 n += 1;
             }
         }
     }
-    wet_s[v] = sum / (float)n;
+    if (DC_IN_BOUNDS(v, g.n(), 2)) wet_s[v] = sum / (float)n;
 }
 
 static dim3 volume_grid(const Grid &g) {
     return dim3((unsigned)((g.nx + 31) / 32), (unsigned)((g.ny + 3) / 4), (unsigned)g.nz);
 }
+
+DC_BOUNDS_TAKE(take_bounds_wet)
 
 void launch_wet_march(DeviceContext &ctx, const Grid &g, const Frame &f, cudaTextureObject_t density,
                       float *wet, cudaStream_t s) {

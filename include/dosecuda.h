@@ -112,6 +112,14 @@ const char *dc_last_error(void);
  * buffers are copied.  No reference counterpart. */
 int dc_host_buffer_mapped(int gpu_id, const void *host, unsigned long long bytes, int *mapped);
 
+/* Debug-build bounds report (no reference counterpart).  A library built
+ * with -DDC_DEBUG_BOUNDS checks the index of every instrumented global
+ * access of the dose kernels against its buffer; the first violation is
+ * recorded (site << 48 | index) and the access skipped.  This call waits for
+ * the device, returns *enabled = 1 for such a build (0 otherwise) and the
+ * first recorded violation since the last call (0: none), and clears it. */
+int dc_debug_bounds(int gpu_id, unsigned long long *violation, int *enabled);
+
 /* ---- Linear dose basis (segment weights of a photon beam) -------------
  * No reference counterpart: the reference's plan loop (plan_imrt.py:140-156)
  * computes each control point's dose and adds it times its output factor.
