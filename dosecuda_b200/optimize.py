@@ -18,6 +18,8 @@ behind ``torch.autograd`` (``engine.proton_dose_autograd``).
   at the objective's voxels only (``ProtonBeamPlan.dose_list`` /
   ``adjoint_list``): the objective and its gradient depend on nothing else,
   and target plus organs at risk are a small part of the grid.
+* ``ImrtOptimizer``: the same loop on the segment (control-point) weights of
+  photon beams, through ``engine.PhotonPlanBasis`` and its adjoint kernel.
 * ``save_influence_csr``/``load_influence_csr``: a dose-influence matrix
   (``ProtonBeamPlan.influence_csr``) cached as ``.npz``."""
 from __future__ import annotations
@@ -217,7 +219,7 @@ class ImptOptimizer:
         if sd.get("version") != 1:
             raise ValueError("unsupported optimiser checkpoint")
         if list(sd["sizes"]) != self.sizes:
-            raise ValueError("checkpoint was written for beams of %s spots, this plan has %s" %
+            raise ValueError("checkpoint was written for beams of %s weights, this plan has %s" %
                              (list(sd["sizes"]), self.sizes))
         with torch.no_grad():
             self.mu.copy_(sd["mu"].to(self.mu.device))
@@ -234,6 +236,50 @@ class ImptOptimizer:
 
     def load(self, path: str):
         self.load_state_dict(torch.load(str(path), map_location="cpu", weights_only=True))
+
+
+class ImrtOptimizer(ImptOptimizer):
+    """Projected Adam on the segment (control-point) weights of photon beams.
+
+    ``bases``: one ``engine.PhotonPlanBasis`` per beam; the plan dose for
+    weights w is sum over beams of ``engine.photon_dose_autograd(w_beam,
+    basis)`` (the basis combination forward, the hand-written adjoint kernel
+    backward), and w = 1 is the plan as delivered (the control-point loop's
+    dose bit for bit).  The loop, the objective, ``scale_to``, checkpoint and
+    resume are ``ImptOptimizer``'s."""
+
+    def __init__(self, bases, objective: DoseObjective, weights: torch.Tensor | None = None,
+                 lr: float | None = None, lr_frac: float = 0.02):
+        self.plans = list(bases)
+        if not self.plans:
+            raise ValueError("at least one photon beam basis is required")
+        self.wets = [None] * len(self.plans)
+        self.objective = objective
+        self.sizes = [int(b.n) for b in self.plans]
+        dev = self.plans[0].device
+        w0 = torch.ones(sum(self.sizes), dtype=torch.float32, device=dev) if weights is None else weights
+        if w0.numel() != sum(self.sizes):
+            raise ValueError("weights must hold one value per control point of all beams")
+        self.mu = w0.detach().to(device=dev, dtype=torch.float32).clone().requires_grad_(True)
+        self.lr = float(lr) if lr is not None else float(lr_frac * self.mu.detach().mean().item())
+        self.opt = torch.optim.Adam([self.mu], lr=self.lr)
+        self.iteration = 0
+        self.value = None
+        self.voxels = "volume"
+        self._list = None
+
+    def dose(self, mu: torch.Tensor | None = None) -> torch.Tensor:
+        """Plan dose of all beams for segment weights ``mu`` (default: the
+        current weights); differentiable."""
+        m = self.mu if mu is None else mu
+        total = None
+        for q, basis in zip(torch.split(m, self.sizes), self.plans):
+            d = engine.photon_dose_autograd(q.contiguous(), basis)
+            total = d if total is None else total + d
+        return total
+
+    def dose_list(self, mu=None):
+        raise NotImplementedError("segment weights are optimised on the full volume")
 
 
 def save_influence_csr(path: str, row_ptr: torch.Tensor, col: torch.Tensor, val: torch.Tensor, shape, n_spots: int):

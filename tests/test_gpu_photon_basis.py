@@ -78,3 +78,28 @@ def test_autograd_matches_finite_differences_and_optimises(arc):
             w.clamp_(min=0.0)
     f1 = objective(engine.photon_dose_autograd(w, basis)).item()
     assert f1 < 0.5 * f0
+
+
+def test_segment_weight_optimiser_and_resume(arc, tmp_path):
+    engine, grid, model, cps, density, basis = arc
+    from dosecuda_b200.optimize import DoseObjective, ImrtOptimizer
+    d1 = basis.dose()
+    target = d1 > 0.5 * float(d1.max())
+    ring = (d1 > 0.1 * float(d1.max())) & ~target
+    obj = DoseObjective().uniform(target, 1.2 * float(d1[target].mean())).max_dose(ring, 0.2 * float(d1.max()), 5.0)
+    opt = ImrtOptimizer([basis], obj)
+    assert torch.equal(opt.dose().detach(), d1)  # unit weights: the plan as delivered
+    f0 = opt.evaluate()
+    opt.run(40)
+    assert opt.evaluate() < 0.7 * f0 and float(opt.mu.detach().min()) >= 0.0
+    # checkpoint / resume continues the run
+    a = ImrtOptimizer([basis], obj)
+    a.run(20)
+    path = str(tmp_path / "imrt.pt")
+    b = ImrtOptimizer([basis], obj)
+    b.run(10, checkpoint=path)
+    c = ImrtOptimizer([basis], obj, weights=torch.full((len(cps),), 3.0, device="cuda"))
+    c.load(path)
+    c.run(10)
+    assert c.iteration == 20
+    assert float((c.mu.detach() - a.mu.detach()).abs().max()) <= 1e-5 * float(a.mu.detach().abs().max())
