@@ -124,3 +124,69 @@ def test_influence_cache_round_trip(tmp_path):
     assert shape == SHAPE and ns == n_spots
     with pytest.raises(ValueError):
         save_influence_csr(path, row_ptr[:-1], col, val, SHAPE, n_spots)
+
+
+def test_objective_on_voxel_list_equals_the_volume_form():
+    plans, wets, obj, target, oar, cold = _case(5)
+    d = torch.rand(SHAPE, dtype=torch.float32) * 3
+    union = obj.voxel_union()
+    assert bool((union[1:] > union[:-1]).all())  # sorted, unique
+    expect = torch.nonzero((target | oar | cold).reshape(-1)).squeeze(1)
+    assert torch.equal(union, expect)
+    assert float(obj.on_list(d.reshape(-1)[union])) == float(obj(d))
+    # a term added later extends the union
+    extra = torch.zeros(SHAPE, dtype=torch.bool)
+    extra[5, 6, 7] = True
+    obj.max_dose(extra, 0.1)
+    assert obj.voxel_union().numel() == union.numel() + 1
+
+
+class DenseBasis:
+    """CPU stand-in for engine.PhotonPlanBasis: per-control-point doses as
+    rows of a dense matrix, output factors, same dose/adjoint interface."""
+
+    def __init__(self, rows: torch.Tensor, of):
+        self.basis = rows
+        self.n = rows.shape[0]
+        self.device = rows.device
+        self.output_factors = torch.tensor(of, dtype=torch.float64)
+
+    def dose(self, weights=None):
+        w = torch.ones(self.n, dtype=torch.float64) if weights is None else weights.detach().double()
+        return (self.basis.double().t() @ (w * self.output_factors)).float().reshape(SHAPE)
+
+    def adjoint(self, grad):
+        return self.output_factors * (self.basis.double() @ grad.reshape(-1).double())
+
+
+def test_imrt_optimiser_and_resume_on_cpu(tmp_path):
+    from dosecuda_b200.optimize import ImrtOptimizer
+    g = torch.Generator().manual_seed(6)
+    n = int(np.prod(SHAPE))
+    bases = [DenseBasis(torch.rand((4, n), generator=g), [1.0, 0.98, 1.02, 1.01]),
+             DenseBasis(torch.rand((3, n), generator=g), [0.97, 1.0, 1.03])]
+    _, _, obj, target, *_ = _case(6)
+    opt = ImrtOptimizer(bases, obj)
+    assert torch.allclose(opt.dose().detach(), bases[0].dose() + bases[1].dose())
+    f0 = opt.evaluate()
+    opt.run(80)
+    assert opt.evaluate() < 0.5 * f0 and float(opt.mu.detach().min()) >= 0.0
+    straight = ImrtOptimizer(bases, obj)
+    straight.run(12)
+    path = str(tmp_path / "imrt.pt")
+    first = ImrtOptimizer(bases, obj)
+    first.run(5, checkpoint=path)
+    resumed = ImrtOptimizer(bases, obj, weights=torch.full((7,), 2.0))
+    resumed.load(path)
+    resumed.run(7)
+    assert torch.equal(resumed.mu.detach(), straight.mu.detach())
+    with pytest.raises(ValueError):
+        ImrtOptimizer(bases[:1], obj).load(path)
+
+
+def test_build_cli_requires_an_output_for_the_checked_variant():
+    import subprocess
+    import sys
+    r = subprocess.run([sys.executable, "-m", "dosecuda_b200.build", "--debug-bounds"], capture_output=True,
+                       text=True, timeout=120)
+    assert r.returncode != 0 and "--out" in r.stderr
