@@ -36,8 +36,14 @@ sys.path.insert(0, ROOT)
 
 PEAKS_FALLBACK = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
 # DRAM bytes (read + write) per launch from one ncu --set full capture of each
-# dominant kernel on these workloads (profiles/*.md)
-NCU_TRAFFIC = {"cccs": 15102976, "pencil_beam": 3622400, "conv_dec0": 67162880 + 26884352}
+# dominant kernel on these workloads, with the summary that records the
+# capture (its command and figures).  A kernel change makes its entry stale
+# until it is captured again.
+NCU_TRAFFIC = {
+    "cccs": (15102976, "profiles/cccs_photon_small.md"),
+    "pencil_beam": (3622400, "profiles/pencil_beam_proton_small.md"),
+    "conv_dec0": (67162880 + 26884352, "profiles/conv_gather_dec0_surrogate_128.md"),
+}
 SM_COUNT = 148
 FP32_LANES_PER_SM = 128
 
@@ -272,23 +278,30 @@ def run_mine(args, ws, rank, local, dist_mod):
     # electron term read once, the dose written once = 16 B per voxel
     cccs_bytes = nvox * 16
 
-    # e2e through the drop-in API (pinned host input, H2D + D2H per call)
+    # e2e through the drop-in API with host numpy in and out, H2D + D2H per
+    # call: the headline passes the pageable array DensityFromHU returns, as
+    # the reference's plan loop does (plan_imrt.py:126-158); the same call
+    # with a page-locked input is reported beside it
+    def e2e_photon(voxels):
+        vol = VolumeObject()
+        vol.voxel_data = voxels
+        vol.origin = np.array(grid.origin, dtype=np.single)
+        vol.spacing = np.array(grid.spacing, dtype=np.single)
+        for _ in range(max(1, args.warmup)):
+            dose_kernels.photon_dose_cuda(model, vol, cp, local)
+        torch.cuda.synchronize()
+        barrier(dist_mod)
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            d = dose_kernels.photon_dose_cuda(model, vol, cp, local)
+        torch.cuda.synchronize()
+        ms = (time.perf_counter() - t0) * 1e3
+        barrier(dist_mod)
+        return aggregate_max(ms, dist_mod), d
+
+    e2e_ms, d = e2e_photon(density)
     pinned = torch.from_numpy(density).pin_memory()
-    vol = VolumeObject()
-    vol.voxel_data = pinned.numpy()
-    vol.origin = np.array(grid.origin, dtype=np.single)
-    vol.spacing = np.array(grid.spacing, dtype=np.single)
-    for _ in range(max(1, args.warmup)):
-        dose_kernels.photon_dose_cuda(model, vol, cp, local)
-    torch.cuda.synchronize()
-    barrier(dist_mod)
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        d = dose_kernels.photon_dose_cuda(model, vol, cp, local)
-    torch.cuda.synchronize()
-    e2e_ms = (time.perf_counter() - t0) * 1e3
-    barrier(dist_mod)
-    e2e_ms = aggregate_max(e2e_ms, dist_mod)
+    e2e_pinned_ms, _ = e2e_photon(pinned.numpy())
     parity_e2e = float(np.abs(d - dose_np).max())
 
     # ---------------- proton (secondary) ----------------
@@ -329,33 +342,39 @@ def run_mine(args, ws, rank, local, dist_mod):
         pairs += int((wet_np <= np.float32(1.1) * r80).sum()) * int((pbeam.spot_list[:, 3].astype(int) == e).sum())
     pb_launches, pb_ms = prof_p.get("pencil_beam", (1, float("nan")))
     pb_avg_ms = pb_ms / max(pb_launches, 1)
-    pb_flops = pairs * 20.0
-    pvol = VolumeObject()
-    pvol.voxel_data = torch.from_numpy(rlsp).pin_memory().numpy()
-    pvol.origin = np.array(pgrid.origin, dtype=np.single)
-    pvol.spacing = np.array(pgrid.spacing, dtype=np.single)
-    for _ in range(max(1, args.warmup)):
-        w = dose_kernels.proton_raytrace_cuda(pmodel, pvol, pbeam, local)
-        wv = VolumeObject()
-        wv.voxel_data, wv.origin, wv.spacing = w, pvol.origin, pvol.spacing
-        dose_kernels.proton_spot_cuda(pmodel, pvol, wv, pbeam, local)
-    barrier(dist_mod)
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        w = dose_kernels.proton_raytrace_cuda(pmodel, pvol, pbeam, local)
-        wv = VolumeObject()
-        wv.voxel_data, wv.origin, wv.spacing = w, pvol.origin, pvol.spacing
-        dose_kernels.proton_spot_cuda(pmodel, pvol, wv, pbeam, local)
-    pe2e_ms = (time.perf_counter() - t0) * 1e3
-    barrier(dist_mod)
-    pe2e_ms = aggregate_max(pe2e_ms, dist_mod)
+    def e2e_proton(voxels):
+        pvol = VolumeObject()
+        pvol.voxel_data = voxels
+        pvol.origin = np.array(pgrid.origin, dtype=np.single)
+        pvol.spacing = np.array(pgrid.spacing, dtype=np.single)
+
+        def beam_call():
+            # the reference's plan loop (plan_impt.py:124-160): WET, then the
+            # dose from a fresh array copy of it
+            w = dose_kernels.proton_raytrace_cuda(pmodel, pvol, pbeam, local)
+            wv = VolumeObject()
+            wv.voxel_data, wv.origin, wv.spacing = np.array(w, dtype=np.single), pvol.origin, pvol.spacing
+            dose_kernels.proton_spot_cuda(pmodel, pvol, wv, pbeam, local)
+
+        for _ in range(max(1, args.warmup)):
+            beam_call()
+        barrier(dist_mod)
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            beam_call()
+        ms = (time.perf_counter() - t0) * 1e3
+        barrier(dist_mod)
+        return aggregate_max(ms, dist_mod)
+
+    pe2e_ms = e2e_proton(rlsp)
+    pe2e_pinned_ms = e2e_proton(torch.from_numpy(rlsp).pin_memory().numpy())
 
     out.update(dict(
         x_ms_per_beam=x_ms_per_beam, t_ms=t_ms, prof_x=prof_x, clocks=clk.summary(), samples=samples,
         n_active=n_active, cccs_avg_ms=cccs_avg_ms, achieved_tf=achieved_tf, fp32_peak=fp32_peak,
-        cccs_bytes=cccs_bytes, e2e_ms=e2e_ms, parity_e2e=parity_e2e, nvox=nvox, pk=pk, pk_kind=pk_kind,
-        spots_per_s=spots_per_s, tp_ms=tp_ms, prof_p=prof_p, pairs=pairs, pb_avg_ms=pb_avg_ms, pb_flops=pb_flops,
-        pe2e_ms=pe2e_ms, n_spots=n_spots, pnvox=rlsp.size,
+        cccs_bytes=cccs_bytes, e2e_ms=e2e_ms, e2e_pinned_ms=e2e_pinned_ms, parity_e2e=parity_e2e, nvox=nvox, pk=pk,
+        pk_kind=pk_kind, spots_per_s=spots_per_s, tp_ms=tp_ms, prof_p=prof_p, pairs=pairs, pb_avg_ms=pb_avg_ms,
+        pe2e_ms=pe2e_ms, pe2e_pinned_ms=pe2e_pinned_ms, n_spots=n_spots, pnvox=rlsp.size,
     ))
     return out
 
@@ -687,7 +706,7 @@ def run_surrogate(args, local, dist_mod):
                      "frac": round(dec0_tf / bf16_peak, 4), "peak_kind": pk_kind + " (cuBLAS bf16)",
                      "kernel_ms": round(t_dec0, 4),
                      "work": "%d FLOPs per launch (2 x voxels x 27 x 16 x 16)" % dec0_flops,
-                     "traffic": NCU_TRAFFIC["conv_dec0"],
+                     "traffic": NCU_TRAFFIC["conv_dec0"][0], "traffic_source": NCU_TRAFFIC["conv_dec0"][1],
                      "stack": {"achieved": round(achieved, 2), "frac": round(achieved / bf16_peak, 4),
                                "work": "%d FLOPs per forward (conv layers from their shapes + head)" % flops}},
         "config": {"workload": "photon surrogate: 128^3 @ 2.5 mm, water body + 1-5 random ellipsoids (HU -900..1500), "
@@ -740,12 +759,40 @@ def cpu_baseline_proton():
     t0 = time.perf_counter()
     wet, march = oracle.proton_wet(rlsp, sp, grid.origin, beam.iso, beam.gantry_angle, beam.couch_angle,
                                    model.VSADX, model.VSADY)
-    oracle.proton_dose(wet.astype(np.float32), sp, grid.origin, beam.iso, beam.gantry_angle, beam.couch_angle,
-                       model, beam.spot_list)
+    _, dense, near = oracle.proton_dose(wet.astype(np.float32), sp, grid.origin, beam.iso, beam.gantry_angle,
+                                        beam.couch_angle, model, beam.spot_list, near_pairs=True)
     dt = time.perf_counter() - t0
     return {"value": round(beam.spot_list.shape[0] / dt, 2), "unit": "spots/s", "cores": oracle.num_threads(),
             "kind": "port",
-            "sample": "one full beam of the 96^3 proton workload (600 spots, FP64 C/OpenMP oracle)"}, march
+            "sample": "one full beam of the 96^3 proton workload (600 spots, FP64 C/OpenMP oracle)"}, march, near
+
+
+def pencil_beam_roofline(r):
+    """The pencil beam's roofline.  Work unit (the algorithmic count, from the
+    oracle): a (voxel, spot) pair within the layer's range whose distance from
+    the spot axis is inside 6 halo sigmas at that voxel, 20 FP32 flops and 2
+    SFU ex2 each.  The kernel culls spots per CTA, so it evaluates somewhat
+    more pairs than that; the dense count (every in-range voxel x every spot of
+    the layer, the reference's work) is reported beside it."""
+    sm_hz = r["pk"].get("sm_max_mhz", 1965.0) * 1e6
+    sec = r["pb_avg_ms"] * 1e-3
+    near = r.get("near_pairs")
+    pairs = near if near else r["pairs"]
+    out = {"bound": "sfu", "kernel": "pencil_beam",
+           "achieved": round(2 * pairs / sec, 1), "peak": round(SM_COUNT * 16 * sm_hz, 1), "unit": "ex2/s",
+           "frac": round(2 * pairs / sec / (SM_COUNT * 16 * sm_hz), 4),
+           "peak_kind": "nominal (148 SMs x 16 SFU lanes x max SM clock); no measured SFU peak exists",
+           "work": ("%d (voxel, spot) pairs inside the cut-off radius (oracle count) x 2 SFU ex2 + 20 FP32 flops"
+                    % pairs) if near else ("%d dense in-range (voxel, spot) pairs (no oracle count: --no-cpu)"
+                                            % pairs),
+           "pairs_per_s": round(pairs / sec, 1), "kernel_ms": round(r["pb_avg_ms"], 4),
+           "fp32": {"achieved_tflops": round(pairs * 20.0 / sec / 1e12, 3), "peak_tflops": round(r["fp32_peak"], 2),
+                    "frac": round(pairs * 20.0 / sec / 1e12 / r["fp32_peak"], 4),
+                    "peak_kind": "nominal FP32 (148 SMs x 128 lanes x 2 x max SM clock)"},
+           "dense": {"pairs": int(r["pairs"]), "pairs_per_s": round(r["pairs"] / sec, 1),
+                     "what": "every in-range voxel x every spot of its layer (the reference's evaluated pairs)"},
+           "traffic": NCU_TRAFFIC["pencil_beam"][0], "traffic_source": NCU_TRAFFIC["pencil_beam"][1]}
+    return out
 
 
 def stage_rates(prof, nvox, march_samples, fetch_rate):
@@ -783,7 +830,7 @@ def main_mine(args):
         march_x = march_p = None
         if ws == 1 and not args.no_cpu:
             cpu_x, oracle_samples, march_x = cpu_baseline_photon()
-            cpu_p, march_p = cpu_baseline_proton()
+            cpu_p, march_p, r["near_pairs"] = cpu_baseline_proton()
             # algorithmic work counted by the oracle (TERMA > 0.01 voxels x cone samples)
             r["achieved_tf"] *= oracle_samples / max(r["samples"], 1)
             r["samples"] = oracle_samples
@@ -813,7 +860,11 @@ def main_mine(args):
                        "parallelism": "replicas" if ws > 1 else "single GPU"},
             "e2e": {"value": round(r["e2e_ms"] / (args.steps * ws), 4), "unit": "ms/beam",
                     "h2d_bytes_per_step": int(r["nvox"] * 4), "d2h_bytes_per_step": int(r["nvox"] * 4),
-                    "api": "dosecuda_b200.dose_kernels.photon_dose_cuda (host numpy in/out; the input pinned by the caller, the returned array page-locked by the call)"},
+                    "api": "dosecuda_b200.dose_kernels.photon_dose_cuda (host numpy in/out: the pageable density "
+                           "array DensityFromHU returns, as the reference's plan loop passes it; the returned "
+                           "array page-locked by the call)",
+                    "pinned_input": {"value": round(r["e2e_pinned_ms"] / (args.steps * ws), 4), "unit": "ms/beam",
+                                     "what": "the same call with a page-locked input array"}},
             # The CCCS's binding unit is the texture pipe (one filtered float2
             # fetch per cone sample; L1TEX ~95 % busy under ncu), so the
             # top-level roof is the fetch rate measured on this GPU by
@@ -839,7 +890,8 @@ def main_mine(args):
                         "peak_kind": r["pk_kind"]},
                 # dram__bytes_read.sum + dram__bytes_write.sum of one ncu capture
                 # of this kernel on this workload (profiles/cccs_photon_small.md)
-                "traffic": NCU_TRAFFIC["cccs"],
+                "traffic": NCU_TRAFFIC["cccs"][0],
+                "traffic_source": NCU_TRAFFIC["cccs"][1],
             },
             "kernels": {k: {"launches": v[0], "total_ms": round(v[1], 4)} for k, v in r["prof_x"].items()},
             "stages": stage_rates(r["prof_x"], r["nvox"], march_x, fetch_rate),
@@ -857,21 +909,13 @@ def main_mine(args):
                            "step": "one beam: WET ray trace + smoothing + pencil-beam dose, RLSP resident in HBM"},
                 "e2e": {"value": round(r["n_spots"] * args.steps * ws / (r["pe2e_ms"] * 1e-3), 1), "unit": "spots/s",
                         "h2d_bytes_per_step": int(r["pnvox"] * 4 * 2), "d2h_bytes_per_step": int(r["pnvox"] * 4 * 2),
-                        "api": "dose_kernels.proton_raytrace_cuda + proton_spot_cuda (host numpy)"},
-                "roofline": {"bound": "fp32", "kernel": "pencil_beam",
-                             "achieved": round(r["pb_flops"] / (r["pb_avg_ms"] * 1e-3) / 1e12, 3),
-                             "peak": round(r["fp32_peak"], 2), "unit": "TFLOP/s",
-                             "frac": round(r["pb_flops"] / (r["pb_avg_ms"] * 1e-3) / 1e12 / r["fp32_peak"], 4),
-                             "work": f"{r['pairs']} (voxel, spot) pairs x 20 FP32 flops (+2 SFU exp each)",
-                             "pairs_per_s": round(r["pairs"] / (r["pb_avg_ms"] * 1e-3), 1),
-                             "kernel_ms": round(r["pb_avg_ms"], 4), "traffic": NCU_TRAFFIC["pencil_beam"],
-                             # two ex2 per pair on the special-function unit (16 per SM and clock)
-                             "sfu": {"achieved_ex2_per_s": round(2 * r["pairs"] / (r["pb_avg_ms"] * 1e-3), 1),
-                                     "peak_ex2_per_s": round(SM_COUNT * 16 * r["pk"].get("sm_max_mhz", 1965.0)
-                                                             * 1e6, 1),
-                                     "frac": round(2 * r["pairs"] / (r["pb_avg_ms"] * 1e-3) /
-                                                   (SM_COUNT * 16 * r["pk"].get("sm_max_mhz", 1965.0) * 1e6), 4),
-                                     "peak_kind": "nominal (148 SMs x 16 SFU lanes x max SM clock)"}},
+                        "api": "dose_kernels.proton_raytrace_cuda + proton_spot_cuda (host numpy: the pageable "
+                               "RLSP array RLSPFromHU returns, the WET passed back as a fresh array copy, as "
+                               "the reference's plan loop does)",
+                        "pinned_input": {"value": round(r["n_spots"] * args.steps * ws / (r["pe2e_pinned_ms"] * 1e-3),
+                                                        1), "unit": "spots/s",
+                                         "what": "the same calls with a page-locked RLSP array"}},
+                "roofline": pencil_beam_roofline(r),
                 "kernels": {k: {"launches": v[0], "total_ms": round(v[1], 4)} for k, v in r["prof_p"].items()},
                 "stages": stage_rates(r["prof_p"], r["pnvox"], march_p, fetch_rate),
                 "gpu_launches": p_launch_per_step * args.steps,
@@ -887,19 +931,35 @@ def main_mine(args):
         dist_mod.destroy_process_group()
 
 
+def load_reference_extension():
+    """The reference's own compiled ``dose_kernels`` extension: the one the
+    reference's package build installed into baseline/_ref (its CMake build,
+    `pip install --target baseline/_ref`), else the same sources built by
+    oracle/build_ref.sh into oracle/_ref.  Returns (module, where)."""
+    import importlib.machinery
+    import importlib.util
+    for where in (os.path.join("baseline", "_ref", "DoseCUDA"), os.path.join("oracle", "_ref")):
+        hits = sorted(glob.glob(os.path.join(ROOT, where, "dose_kernels*.so")))
+        if hits:
+            loader = importlib.machinery.ExtensionFileLoader("dose_kernels", hits[0])
+            spec = importlib.util.spec_from_file_location("dose_kernels", hits[0], loader=loader)
+            mod = importlib.util.module_from_spec(spec)
+            loader.exec_module(mod)
+            return mod, os.path.relpath(hits[0], ROOT)
+    return None, None
+
+
 # ----------------------------------------------------------------------------
 def main_reference(args):
     """The reference DoseCUDA CUDA extension through its own API, same inputs."""
     ws, rank, local = dist_env()
     if rank != 0:
         return
-    ref_dir = os.path.join(ROOT, "oracle", "_ref")
-    if not glob.glob(os.path.join(ref_dir, "dose_kernels*.so")):
-        print(json.dumps({"impl": "reference", "unavailable": "reference build oracle/_ref missing "
-                                                               "(oracle/build_ref.sh needs the reference sources)"}))
+    ref, ref_origin = load_reference_extension()
+    if ref is None:
+        print(json.dumps({"impl": "reference", "unavailable": "no reference build: neither baseline/_ref (pip install "
+                                                               "of the reference) nor oracle/_ref (oracle/build_ref.sh)"}))
         return
-    sys.path.insert(0, ref_dir)
-    import dose_kernels as ref  # the reference build
     from dosecuda_b200.plan import VolumeObject
 
     grid, model, cp, density = photon_workload()
@@ -987,9 +1047,10 @@ def main_reference(args):
                    "parallelism": "single GPU"},
         "e2e": {"value": round(x_ms, 4), "unit": "ms/beam", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "cpu_baseline": {"value": round(x_ms, 4), "unit": "ms/beam", "cores": 1, "kind": "reference",
-                         "sample": "the reference's own implementation is CUDA-only: its extension built from the "
-                                   "reference sources for sm_100a, run on the B200 through its Python API with "
-                                   "host numpy buffers (its per-call allocation and copies included)"},
+                         "sample": "the reference's own implementation is CUDA-only: its extension (%s) built from "
+                                   "the reference sources for sm_100a, run on the B200 through its Python API with "
+                                   "host numpy buffers (its per-call allocation and copies included)" % ref_origin},
+        "reference_build": ref_origin,
         "clocks": clk.summary(),
         "secondary": {"metric": "IMPT spots/s", "value": round(n_spots / p_s, 1), "unit": "spots/s",
                       "higher_is_better": True, "ms_per_step": round(p_s * 1e3, 4),

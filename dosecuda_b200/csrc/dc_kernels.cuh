@@ -79,6 +79,7 @@ unsigned long long take_bounds_wet();
 unsigned long long take_bounds_photon();
 unsigned long long take_bounds_proton();
 unsigned long long take_bounds_basis();
+unsigned long long take_bounds_noalloc();
 
 // Builds the sorted spot table and the layer table on the host.  Throws
 // Error(DC_ERR_VALUE) for malformed input.

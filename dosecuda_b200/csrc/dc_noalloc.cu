@@ -10,23 +10,31 @@
 // dc_proton_raytrace_dev — the 1 mm ray march to the source followed by the
 // beam's-eye-view smoothing — but:
 //  * its only scratch, the unsmoothed WET volume, is the file-scope device
-//    array g_noalloc_wet below (kNoAllocMaxVoxels floats = 16 MiB), which
-//    every GPU that loads the library holds until the process exits;
+//    array g_noalloc_wet below (kNoAllocMaxVoxels floats = 16 MiB).  CUDA
+//    commits it on a device when the library's device code is loaded there,
+//    which with lazy module loading (the CUDA 12 default) is the first call of
+//    this entry point on that device; from then on the device holds it until
+//    the process exits.  That first call can therefore fail with an
+//    out-of-memory status on a full device, and should come before any stream
+//    capture;
 //  * it samples the caller's linear RLSP buffer with its own trilinear
 //    interpolation (border value 0, interpolation weights rounded to 1/256
 //    as the texture unit does) instead of building a cudaArray and a
 //    texture object, so its WET can differ from the texture path by
 //    rounding of the weights (a few 1e-4 cm);
 //  * it creates no stream, event or context state: the kernels go on the
-//    caller's stream.
+//    caller's stream, and the caller's current device is restored on return.
 // The host code never dereferences g_noalloc_wet (in host code the name is
-// only a stand-in, not a device address): the first call on each device looks
-// up the array's device address with cudaGetSymbolAddress, with that device
-// current, and every call passes that pointer to the kernels.  Make that first
-// call on a device before any stream capture.  The march writes every voxel of
-// the scratch it uses before the smoothing reads it, so nothing needs
-// clearing between calls.
+// only a stand-in, not a device address): the first call in each CUDA context
+// looks up the array's device address with cudaGetSymbolAddress, with that
+// device current, and every call passes that pointer to the kernels.  The
+// lookup is keyed by the context's unique id, so a device reset
+// (cudaDeviceReset, which replaces the context and may move the array) makes
+// the next call look it up again.  The march writes every voxel of the
+// scratch it uses before the smoothing reads it, so nothing needs clearing
+// between calls.
 #include <cmath>
+#include <cuda.h>
 #include <mutex>
 #include <string>
 
@@ -40,6 +48,8 @@ namespace dc {
 __global__ void wet_smooth_kernel(Grid g, Frame f, const float *__restrict__ wet, float *__restrict__ wet_s);
 
 constexpr long long kNoAllocMaxVoxels = 4LL << 20;  // 4,194,304 voxels
+
+DC_BOUNDS_WORD
 
 // Unsmoothed WET of the last call.  Every call overwrites the voxels it uses
 // before reading them; calls that overlap on the GPU (two streams, two host
@@ -69,8 +79,10 @@ __device__ __forceinline__ float linear_fetch(const float *__restrict__ v, const
             for (int di = 0; di < 2; ++di) {
                 const int i = i0 + di;
                 const float w = (di ? a : 1.0f - a) * wyz;
-                if ((unsigned)i < (unsigned)g.nx && (unsigned)j < (unsigned)g.ny && (unsigned)k < (unsigned)g.nz)
-                    r = fmaf(w, __ldg(v + (long long)i + (long long)g.nx * (j + (long long)g.ny * k)), r);
+                if ((unsigned)i < (unsigned)g.nx && (unsigned)j < (unsigned)g.ny && (unsigned)k < (unsigned)g.nz) {
+                    const long long idx = (long long)i + (long long)g.nx * (j + (long long)g.ny * k);
+                    if (DC_IN_BOUNDS(idx, g.n(), 1)) r = fmaf(w, __ldg(v + idx), r);
+                }
             }
         }
     }
@@ -98,26 +110,81 @@ __global__ void __launch_bounds__(128) wet_march_linear_kernel(Grid g, Frame f, 
         wet_sum = fmaf(fmaxf(linear_fetch(rho, g, tc), 0.0f), 0.1f, wet_sum);
         t += 1.0f;
     }
-    wet[(long long)i + (long long)g.nx * (j + (long long)g.ny * k)] = wet_sum;
+    const long long v = (long long)i + (long long)g.nx * (j + (long long)g.ny * k);
+    if (DC_IN_BOUNDS(v, kNoAllocMaxVoxels, 2)) wet[v] = wet_sum;
 }
+
+DC_BOUNDS_TAKE(take_bounds_noalloc)
 
 namespace {
 
 constexpr int kNoAllocMaxDevices = 64;
 std::mutex g_symbol_mu;
-float *g_symbol_ptr[kNoAllocMaxDevices] = {nullptr};
+struct SymbolCache {
+    unsigned long long ctx_id = 0;  // unique id of the context the address belongs to (0: none)
+    float *ptr = nullptr;
+};
+SymbolCache g_symbol[kNoAllocMaxDevices];
 
-// Device address of g_noalloc_wet on the current device `dev`, looked up once.
+using CtxGetCurrentFn = CUresult (*)(CUcontext *);
+using CtxGetIdFn = CUresult (*)(CUcontext, unsigned long long *);
+
+template <class Fn>
+Fn driver_entry(const char *name) {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    if (cudaGetDriverEntryPoint(name, &p, cudaEnableDefault, &q) != cudaSuccess || q != cudaDriverEntryPointSuccess) {
+        (void)cudaGetLastError();
+        return nullptr;
+    }
+    return reinterpret_cast<Fn>(p);
+}
+
+// Unique id of the calling thread's current CUDA context (made current by the
+// runtime call before this one).  Ids are never reused within a process, so a
+// context created after a device reset gets a new one.
+unsigned long long current_context_id() {
+    static const CtxGetCurrentFn get_current = driver_entry<CtxGetCurrentFn>("cuCtxGetCurrent");
+    static const CtxGetIdFn get_id = driver_entry<CtxGetIdFn>("cuCtxGetId");
+    if (!get_current || !get_id) throw Error(DC_ERR_CUDA, "cuCtxGetCurrent/cuCtxGetId unavailable in this driver");
+    CUcontext c = nullptr;
+    unsigned long long id = 0;
+    if (get_current(&c) != CUDA_SUCCESS || c == nullptr || get_id(c, &id) != CUDA_SUCCESS)
+        throw Error(DC_ERR_CUDA, "no current CUDA context after cudaSetDevice");
+    return id;
+}
+
+// Device address of g_noalloc_wet in the current context of device `dev`,
+// looked up once per context.
 float *scratch_for(int dev) {
+    // cudaSetDevice (CUDA 12 and later) has made the device's primary context
+    // current on this thread.
+    const unsigned long long id = current_context_id();
     std::lock_guard<std::mutex> lk(g_symbol_mu);
-    if (!g_symbol_ptr[dev]) {
+    SymbolCache &c = g_symbol[dev];
+    if (c.ptr == nullptr || c.ctx_id != id) {
         float *p = nullptr;
         cudaError_t e = cudaGetSymbolAddress((void **)&p, g_noalloc_wet);
         if (e != cudaSuccess) throw_cuda(e, "cudaGetSymbolAddress(g_noalloc_wet)");
-        g_symbol_ptr[dev] = p;
+        c.ptr = p;
+        c.ctx_id = id;
     }
-    return g_symbol_ptr[dev];
+    return c.ptr;
 }
+
+// Restores the calling thread's current device when the entry point returns.
+struct CurrentDeviceGuard {
+    int saved = -1;
+    CurrentDeviceGuard() {
+        if (cudaGetDevice(&saved) != cudaSuccess) {
+            (void)cudaGetLastError();
+            saved = -1;
+        }
+    }
+    ~CurrentDeviceGuard() {
+        if (saved >= 0) (void)cudaSetDevice(saved);
+    }
+};
 
 int fail(int code, const std::string &msg) {
     set_last_error(msg);
@@ -149,6 +216,7 @@ extern "C" int dc_proton_raytrace_noalloc(int gpu_id, const float *rlsp_dev, int
     if (e != cudaSuccess) return fail(DC_ERR_CUDA, cudaGetErrorString(e));
     if (gpu_id < 0 || gpu_id >= count || gpu_id >= kNoAllocMaxDevices)
         return fail(DC_ERR_CUDA, cudaGetErrorString(cudaErrorInvalidDevice));
+    CurrentDeviceGuard keep_device;
     try {
         DC_CUDA(cudaSetDevice(gpu_id));
         float *scratch = scratch_for(gpu_id);

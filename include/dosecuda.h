@@ -188,9 +188,14 @@ int dc_proton_raytrace_dev(int gpu_id,
  * library, held by every GPU that loads it until the process exits; larger
  * volumes are rejected with DC_ERR_VALUE.  The RLSP is read from the
  * caller's device buffer (no texture), the output goes to the caller's
- * device buffer, work is enqueued on `stream`.  The first call on a device
- * looks up the scratch address — make it before any stream capture.  All
- * calls share the scratch: calls that overlap on the GPU race. */
+ * device buffer, work is enqueued on `stream`.  The scratch is committed
+ * on a device when the library's device code is loaded there, which under
+ * CUDA's default lazy module loading is the first call on that device: that
+ * call may fail with DC_ERR_CUDA (out of memory) on a full device, and it
+ * looks up the scratch address, so make it before any stream capture (the
+ * lookup is repeated once after a device reset).  The calling thread's
+ * current device is restored on return.  All calls share the scratch:
+ * calls that overlap on the GPU race. */
 int dc_proton_raytrace_noalloc(int gpu_id,
                                const float *rlsp_dev, int nz, int ny, int nx,
                                const float spacing[3], const float origin[3],

@@ -5,7 +5,7 @@ single-threaded build when no OpenMP runtime links.  Also (re)builds the
 reference CUDA extension into oracle/_ref/ when the reference sources are
 present (oracle/build_ref.sh).
 
-    python oracle/build.py [--ref]
+    python oracle/build.py [--ref [REFERENCE_ROOT]]
 """
 from __future__ import annotations
 
@@ -45,16 +45,31 @@ def build_oracle(force: bool = False) -> str:
     raise RuntimeError("could not build the oracle:\n" + "\n".join(errors))
 
 
-def build_reference() -> bool:
-    """Build oracle/_ref/dose_kernels*.so from the reference sources if they
-    are present; returns False when they are not."""
+def reference_root(explicit: str | None = None) -> str | None:
+    """The reference checkout: the argument, else $DOSECUDA_REFERENCE, else a
+    ``reference`` directory beside this repository; None when none of these
+    holds the reference sources."""
+    repo = os.path.dirname(HERE)
+    for cand in (explicit, os.environ.get("DOSECUDA_REFERENCE"), os.path.join(os.path.dirname(repo), "reference")):
+        if cand and os.path.isdir(os.path.join(cand, "DoseCUDA", "dose_kernels")):
+            return cand
+    return None
+
+
+def build_reference(root: str | None = None) -> bool:
+    """Build the reference checker into oracle/_ref/ (its CPython extension and
+    the TERMA harness) from the reference sources if they are present;
+    returns False when they are not."""
     script = os.path.join(HERE, "build_ref.sh")
-    ref_root = os.environ.get("DOSECUDA_REFERENCE", "/root/reference")
-    if not os.path.isdir(os.path.join(ref_root, "DoseCUDA", "dose_kernels")):
+    ref_root = reference_root(root)
+    if ref_root is None:
         return False
     ref_dir = os.path.join(HERE, "_ref")
-    so = [f for f in os.listdir(ref_dir)] if os.path.isdir(ref_dir) else []
-    if any(f.startswith("dose_kernels") and f.endswith(".so") for f in so):
+    have = set(os.listdir(ref_dir)) if os.path.isdir(ref_dir) else set()
+    newest_src = max(os.path.getmtime(script), os.path.getmtime(os.path.join(HERE, "ref_terma.cu")))
+    ok = (any(f.startswith("dose_kernels") and f.endswith(".so") for f in have) and "libref_terma.so" in have
+          and os.path.getmtime(os.path.join(ref_dir, "libref_terma.so")) >= newest_src)
+    if ok:
         return True
     subprocess.run(["bash", script, ref_root], check=True, env=dict(os.environ, PYTHON=sys.executable))
     return True
@@ -63,4 +78,5 @@ def build_reference() -> bool:
 if __name__ == "__main__":
     print(build_oracle(force="--force" in sys.argv))
     if "--ref" in sys.argv:
-        print("reference built:", build_reference())
+        i = sys.argv.index("--ref")
+        print("reference built:", build_reference(sys.argv[i + 1] if len(sys.argv) > i + 1 else None))

@@ -31,7 +31,7 @@
  *   cccKernel             IMRTClasses.cu:252-350 (+ kernelTilt :173-203)
  *   Texture3D sampler     DoseCUDA/dose_kernels/TextureClasses.cu:5-38
  *
- * Build: oracle/Makefile (gcc -O2 -fopenmp -ffp-contract=off).
+ * Build: oracle/build.py (gcc -O2 -fopenmp -ffp-contract=off).
  */
 #include <math.h>
 #include <stdlib.h>
@@ -310,6 +310,8 @@ static int spot_cmp(const void *a, const void *b) {
  * as the reference receives it (float).  Returns the number of
  * (voxel, spot) pairs evaluated (voxels inside the layer's range), or -1 on
  * an invalid energy id. */
+static long g_last_near_pairs = 0;
+
 long oracle_proton_dose(const float *wet, int nz, int ny, int nx, const float spacing[3], const float origin[3],
                         const float iso[3], double gantry, float couch, float vsadx, float vsady,
                         const float *dvp, int n_energies, int dvp_len, const float *lut_d, const float *lut_s,
@@ -336,9 +338,9 @@ long oracle_proton_dose(const float *wet, int nz, int ny, int nx, const float sp
     for (int s = 0; s < n_spots; ++s)
         if (s == 0 || sp[s].e != sp[s - 1].e) ls[nl++] = s;
     ls[nl] = n_spots;
-    long pairs = 0;
+    long pairs = 0, near = 0;
     double VX = vsadx, VY = vsady;
-#pragma omp parallel for collapse(2) schedule(dynamic, 2) reduction(+ : pairs)
+#pragma omp parallel for collapse(2) schedule(dynamic, 2) reduction(+ : pairs, near)
     for (int k = 0; k < nz; ++k)
         for (int j = 0; j < ny; ++j)
             for (int i = 0; i < nx; ++i) {
@@ -384,7 +386,7 @@ long oracle_proton_dose(const float *wet, int nz, int ny, int nx, const float sp
                     double pfac = (1.0 - hw) * idd / (2.0 * M_PI * st * st);
                     double hfac = hw * idd / (2.0 * M_PI * sht * sht);
                     double ps = -0.5 / (st * st), hsc = -0.5 / (sht * sht);
-                    double acc = 0.0;
+                    double acc = 0.0, reach2 = 36.0 * sht * sht;
                     for (int s = ls[l]; s < ls[l + 1]; ++s) {
                         double tx = sp[s].x / VX, ty = sp[s].y / VY;
                         double rx = h.x - sp[s].x, ry = h.y - sp[s].y, rz = h.z;
@@ -393,6 +395,7 @@ long oracle_proton_dose(const float *wet, int nz, int ny, int nx, const float sp
                         double dot = tx * rx + ty * ry - rz;
                         double r2 = ray2 - dot * dot / t2;
                         acc += sp[s].mu * (pfac * exp(ps * r2) + hfac * exp(hsc * r2));
+                        near += r2 <= reach2;
                     }
                     pairs += ls[l + 1] - ls[l];
                     total += acc;
@@ -401,8 +404,14 @@ long oracle_proton_dose(const float *wet, int nz, int ny, int nx, const float sp
             }
     free(ls);
     free(sp);
+    g_last_near_pairs = near;
     return pairs;
 }
+
+/* (voxel, spot) pairs of the last oracle_proton_dose call whose distance from
+ * the spot's axis is within 6 halo sigmas at the voxel (6 * sqrt(sigma_tot^2 +
+ * sigma_halo^2)): the pencil beam's work unit inside its cut-off radius. */
+long oracle_last_near_pairs(void) { return g_last_near_pairs; }
 
 /* ------------------------------------------------------------- photon */
 typedef struct {
@@ -434,6 +443,28 @@ static double head_transmission(const photon_model_t *m, const mlc_t *mlc, d3 p,
         t += 0.5 * (erf(t2 * k) - erf(t1 * k)) * 0.5 * (erf(e2 * k) - erf(e1 * k));
     }
     return t;
+}
+
+/* Primary and scatter head transmission at every voxel centre
+ * (headTransmission, IMRTClasses.cu:120-150, as called by termaKernel
+ * :209-250), in double.  Tests use it to locate voxels whose primary
+ * transmission vanishes, where the reference's TERMA divides by it. */
+void oracle_photon_transmission(int nz, int ny, int nx, const float spacing[3], const float origin[3],
+                                const photon_model_t *m, const float iso[3], double gantry, float coll, float couch,
+                                const mlc_t *mlc, double *tp_out, double *ts_out) {
+    grid_t g = make_grid(nz, ny, nx, spacing);
+    frame_t f = make_frame(iso, origin, gantry, couch, coll, m->psd);
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int k = 0; k < nz; ++k)
+        for (int j = 0; j < ny; ++j)
+            for (int i = 0; i < nx; ++i) {
+                long v = i + (long)nx * (j + (long)ny * k);
+                f3 pf = voxel_xyz(&g, &f, i, j, k);
+                d3 p = {pf.x, pf.y, pf.z};
+                d3 h = image_to_head_d(&f, p, 1);
+                tp_out[v] = head_transmission(m, mlc, h, m->psd, m->pss);
+                ts_out[v] = head_transmission(m, mlc, h, m->ssd, m->sss);
+            }
 }
 
 /* Photon dose of one control point (IMRTClasses.cu:209-405).  terma/electron

@@ -52,6 +52,11 @@ def load():
         lib.oracle_photon_dose.argtypes = vol + [C.POINTER(_PhotonModel), F3, C.c_float, C.c_double, C.c_float,
                                                  C.c_float, C.POINTER(_Mlc), C.c_int, C.c_void_p, C.c_void_p,
                                                  C.c_void_p]
+        lib.oracle_photon_transmission.restype = None
+        lib.oracle_photon_transmission.argtypes = [C.c_int, C.c_int, C.c_int, F3, F3, C.POINTER(_PhotonModel), F3,
+                                                   C.c_double, C.c_float, C.c_float, C.POINTER(_Mlc), C.c_void_p,
+                                                   C.c_void_p]
+        lib.oracle_last_near_pairs.restype = C.c_long
         lib.oracle_num_threads.restype = C.c_int
         _lib = lib
     return _lib
@@ -87,9 +92,10 @@ def proton_wet(rlsp, spacing, origin, iso, gantry, couch, vsadx, vsady, tex_mode
     return (wet, wraw, n) if raw else (wet, n)
 
 
-def proton_dose(wet, spacing, origin, iso, gantry, couch, model, spots):
+def proton_dose(wet, spacing, origin, iso, gantry, couch, model, spots, near_pairs=False):
     """Pencil-beam dose (float64) from a float32 smoothed WET; returns
-    (dose, evaluated (voxel, spot) pairs)."""
+    (dose, evaluated (voxel, spot) pairs), with near_pairs=True also the
+    pairs within 6 halo sigmas of the spot axis."""
     w = _c(wet)
     nz, ny, nx = w.shape
     dvp = _c(model.divergence_params)
@@ -103,15 +109,12 @@ def proton_dose(wet, spacing, origin, iso, gantry, couch, model, spots):
                                   dvp.shape[1], _p(ld), _p(ls), _p(li), ld.shape[1], _p(sp), sp.shape[0], _p(dose))
     if n < 0:
         raise ValueError("spot energy id outside the beam model")
+    if near_pairs:
+        return dose, n, load().oracle_last_near_pairs()
     return dose, n
 
 
-def photon_dose(density, spacing, origin, model, iso, mu, gantry, collimator, couch, mlc, tex_mode=0,
-                intermediates=False):
-    """CCCS dose (float64) of one control point; returns (dose, samples) or,
-    with intermediates=True, (dose, terma, electron, samples)."""
-    d = _c(density)
-    nz, ny, nx = d.shape
+def _photon_structs(model, mlc):
     keep = {}
 
     def fp(name, arr):
@@ -139,10 +142,83 @@ def photon_dose(density, spacing, origin, model, iso, mu, gantry, collimator, co
     mm = _Mlc()
     mm.n_pairs = ml.shape[0]
     mm.x1, mm.x2, mm.yoff, mm.yw = (fp("m%d" % c, ml[:, c]) for c in range(4))
+    return m, mm, keep
+
+
+def photon_dose(density, spacing, origin, model, iso, mu, gantry, collimator, couch, mlc, tex_mode=0,
+                intermediates=False):
+    """CCCS dose (float64) of one control point; returns (dose, samples) or,
+    with intermediates=True, (dose, terma, electron, samples)."""
+    d = _c(density)
+    nz, ny, nx = d.shape
+    m, mm, keep = _photon_structs(model, mlc)
     dose = np.empty(d.shape, np.float64)
     terma = np.empty(d.shape, np.float64)
     elec = np.empty(d.shape, np.float64)
     n = load().oracle_photon_dose(_p(d), nz, ny, nx, _f3(spacing), _f3(origin), C.byref(m), _f3(iso), float(mu),
                                   float(gantry), float(collimator), float(couch), C.byref(mm), int(tex_mode),
                                   _p(terma), _p(elec), _p(dose))
+    del keep
     return (dose, terma, elec, n) if intermediates else (dose, n)
+
+
+def photon_transmission(shape, spacing, origin, model, iso, gantry, collimator, couch, mlc):
+    """Primary and scatter head transmission (float64) at every voxel centre."""
+    nz, ny, nx = shape
+    m, mm, keep = _photon_structs(model, mlc)
+    tp = np.empty(shape, np.float64)
+    ts = np.empty(shape, np.float64)
+    load().oracle_photon_transmission(nz, ny, nx, _f3(spacing), _f3(origin), C.byref(m), _f3(iso), float(gantry),
+                                      float(collimator), float(couch), C.byref(mm), _p(tp), _p(ts))
+    del keep
+    return tp, ts
+
+
+# ---------------------------------------------------------------------------
+# The reference's own ray-trace + TERMA kernels (oracle/_ref/libref_terma.so,
+# built from the reference sources by build_ref.sh; needs a GPU to run).
+# ---------------------------------------------------------------------------
+_ref_terma = None
+
+
+def reference_terma_available() -> bool:
+    return os.path.exists(os.path.join(HERE, "_ref", "libref_terma.so"))
+
+
+def reference_photon_terma(density, spacing, origin, model, iso, mu, gantry, collimator, couch, mlc, gpu_id=0):
+    """(WET, TERMA, electron) float32 volumes of one control point from the
+    reference's rayTraceKernel and termaKernel (CudaClasses.cu:180-228,
+    IMRTClasses.cu:209-250)."""
+    global _ref_terma
+    if _ref_terma is None:
+        lib = C.CDLL(os.path.join(HERE, "_ref", "libref_terma.so"))
+        F3 = C.c_float * 3
+        lib.ref_photon_terma.restype = C.c_int
+        lib.ref_photon_terma.argtypes = ([C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_float, F3, F3,
+                                          C.c_float, C.c_float, C.c_float, C.c_void_p] +
+                                         [C.c_int] + [C.c_void_p] * 3 + [C.c_int] + [C.c_void_p] * 3 +
+                                         [C.c_int] + [C.c_void_p] * 4 + [C.c_float] + [C.c_void_p] * 3 +
+                                         [C.c_char_p, C.c_int])
+        _ref_terma = lib
+    d = _c(density)
+    nz, ny, nx = d.shape
+    scal = _c([model.mu_calibration, model.primary_source_distance, model.scatter_source_distance,
+               model.primary_source_size, model.scatter_source_size, model.mlc_distance,
+               model.scatter_source_weight, model.electron_attenuation, model.electron_source_weight,
+               model.electron_fitted_dmax])
+    pr, pi, ps = (_c(getattr(model, k)) for k in ("profile_radius", "profile_intensities", "profile_softening"))
+    sm, spw, ssw = (_c(getattr(model, k)) for k in ("spectrum_attenuation_coefficients", "spectrum_primary_weights",
+                                                     "spectrum_scatter_weights"))
+    ml = np.asarray(mlc, np.float32)
+    cols = [_c(ml[:, c]) for c in range(4)]
+    wet = np.empty(d.shape, np.float32)
+    terma = np.empty(d.shape, np.float32)
+    elec = np.empty(d.shape, np.float32)
+    err = C.create_string_buffer(512)
+    rc = _ref_terma.ref_photon_terma(int(gpu_id), _p(d), nz, ny, nx, float(spacing), _f3(origin), _f3(iso),
+                                     float(gantry), float(collimator), float(couch), _p(scal), len(pr), _p(pr),
+                                     _p(pi), _p(ps), len(sm), _p(sm), _p(spw), _p(ssw), ml.shape[0],
+                                     *[_p(c) for c in cols], float(mu), _p(wet), _p(terma), _p(elec), err, 512)
+    if rc != 0:
+        raise RuntimeError("reference TERMA harness: " + err.value.decode())
+    return wet, terma, elec

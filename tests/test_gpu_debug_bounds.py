@@ -47,6 +47,12 @@ out["adj"] = bp.adjoint(wt, g).cpu().numpy()
 vox = torch.tensor([-5, 0, 7, wt.numel() - 1, wt.numel(), 123456789], dtype=torch.int32, device="cuda")
 out["list"] = bp.dose_list(wt, vox).cpu().numpy()
 out["list_adj"] = bp.adjoint_list(wt, vox, torch.ones(vox.numel(), device="cuda")).cpu().numpy()
+nw = torch.empty_like(rlt := torch.as_tensor(rl.voxel_data).cuda())
+_lib.raise_for(lib.dc_proton_raytrace_noalloc(0, C.c_void_p(rlt.data_ptr()), *rlt.shape, _lib.f3(pg.spacing),
+                                              _lib.f3(pg.origin), _lib.f3(pb.iso), float(pb.gantry_angle),
+                                              float(pb.couch_angle), float(pm.VSADX), float(pm.VSADY),
+                                              C.c_void_p(nw.data_ptr()), C.c_void_p(0)))
+out["noalloc_wet"] = nw.cpu().numpy()
 r, c, v = bp.influence_csr(wt, cutoff=1e-4)
 out["csr_r"], out["csr_c"], out["csr_v"] = r.cpu().numpy(), c.cpu().numpy(), v.cpu().numpy()
 torch.cuda.synchronize()

@@ -70,9 +70,19 @@ def test_noalloc_matches_existing_entry_point_on_two_calls():
     # the shared scratch keeps the previous call's contents; a repeat of the
     # first call must not see them
     out_a2 = torch.full_like(t, -1.0)
-    assert _noalloc_wet(lib, t, grid, beam_a, model, stream, out_a2) == _lib.DC_OK
+    # after the first call (which commits the scratch) further calls leave
+    # the device's free memory and torch's pool untouched, and the calling
+    # thread's current device as it was
     torch.cuda.synchronize()
+    free0, reserved0, dev0 = torch.cuda.mem_get_info()[0], torch.cuda.memory_reserved(), torch.cuda.current_device()
+    assert _noalloc_wet(lib, t, grid, beam_a, model, stream, out_a2) == _lib.DC_OK
+    assert _noalloc_wet(lib, t, grid, beam_b, model, stream, out_b) == _lib.DC_OK
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info()[0] == free0
+    assert torch.cuda.memory_reserved() == reserved0
+    assert torch.cuda.current_device() == dev0
     assert torch.equal(out_a2, out_a)
+    assert _close(out_b.cpu().numpy(), ref_b.cpu().numpy())
 
 
 def test_noalloc_rejects_volumes_beyond_its_scratch():
