@@ -263,6 +263,8 @@ def run_mine(args, ws, rank, local, dist_mod):
     torch.cuda.synchronize()
     prof_x = _lib.profile_read(local)
     _lib.raise_for(lib.dc_profile_enable(local, 0))
+    depth_mode = engine.photon_depth_mode(local)
+    depth_marched = engine.photon_depth_marched(local)
     dose_np = dose_t.cpu().numpy()
     # active voxels = TERMA > 0.01 (the voxels the CCCS evaluates); from the
     # engine's TERMA mask we only need the count, taken as dose > 0 voxels.
@@ -370,7 +372,7 @@ def run_mine(args, ws, rank, local, dist_mod):
     pe2e_pinned_ms = e2e_proton(torch.from_numpy(rlsp).pin_memory().numpy())
 
     out.update(dict(
-        x_ms_per_beam=x_ms_per_beam, t_ms=t_ms, prof_x=prof_x, clocks=clk.summary(), samples=samples,
+        x_ms_per_beam=x_ms_per_beam, t_ms=t_ms, prof_x=prof_x, depth_mode=depth_mode, depth_marched=depth_marched, clocks=clk.summary(), samples=samples,
         n_active=n_active, cccs_avg_ms=cccs_avg_ms, achieved_tf=achieved_tf, fp32_peak=fp32_peak,
         cccs_bytes=cccs_bytes, e2e_ms=e2e_ms, e2e_pinned_ms=e2e_pinned_ms, parity_e2e=parity_e2e, nvox=nvox, pk=pk,
         pk_kind=pk_kind, spots_per_s=spots_per_s, tp_ms=tp_ms, prof_p=prof_p, pairs=pairs, pb_avg_ms=pb_avg_ms,
@@ -816,6 +818,19 @@ def stage_rates(prof, nvox, march_samples, fetch_rate):
     return out
 
 
+def depth_stage(r):
+    """The photon radiological-depth pass of one step: its mode, its kernels'
+    total time and, for the lattice, the voxels that fell back to the exact
+    march."""
+    names = [k for k in r["prof_x"] if k.startswith("xray_") or k == "wet_march"]
+    ms = sum(r["prof_x"][k][1] / max(r["prof_x"][k][0], 1) for k in names)
+    out = {"mode": r["depth_mode"], "kernels": names, "ms": round(ms, 4)}
+    if r["depth_mode"] == "lattice" and r["depth_marched"] >= 0:
+        out["voxels_marched_exactly"] = int(r["depth_marched"])
+        out["marched_frac"] = round(r["depth_marched"] / r["nvox"], 5)
+    return out
+
+
 def main_mine(args):
     import torch
     ws, rank, local = dist_env()
@@ -838,8 +853,10 @@ def main_mine(args):
         hbm = pk.get("hbm_gbs", PEAKS_FALLBACK["hbm_gbs"])
         tex = texture_roof(local, r["samples"] / (r["cccs_avg_ms"] * 1e-3))
         fetch_rate = tex["peak"] if tex else None
-        x_launch_per_step = 4  # wet_march, terma, cone_dirs, cccs
-        p_launch_per_step = 3  # wet_march, wet_smooth, pencil_beam
+        # this library's kernels per step: the profiled ones (depth pass, TERMA,
+        # CCCS) plus the unprofiled one-block cone-direction kernel
+        x_launch_per_step = sum(v[0] for v in r["prof_x"].values()) // max(args.steps, 1) + 1
+        p_launch_per_step = sum(v[0] for v in r["prof_p"].values()) // max(args.steps, 1)
         line = {
             "metric": "CCCS ms/beam",
             "value": round(r["x_ms_per_beam"], 4),
@@ -895,6 +912,7 @@ def main_mine(args):
             },
             "kernels": {k: {"launches": v[0], "total_ms": round(v[1], 4)} for k, v in r["prof_x"].items()},
             "stages": stage_rates(r["prof_x"], r["nvox"], march_x, fetch_rate),
+            "depth_pass": depth_stage(r),
             "gpu_launches": x_launch_per_step * args.steps,
             "clocks": r["clocks"],
             "cpu_baseline": cpu_x,

@@ -55,6 +55,11 @@ class PhotonModel(C.Structure):
     ]
 
 
+class FluenceMap(C.Structure):
+    """dc_fluence_map: beamlet grid on the beam's-eye-view isocentre plane."""
+    _fields_ = [("na", C.c_int), ("nb", C.c_int), ("a0", C.c_float), ("b0", C.c_float), ("pitch", C.c_float)]
+
+
 class ControlPoint(C.Structure):
     """Mirror of ``dc_control_point``."""
     _fields_ = [
@@ -79,6 +84,9 @@ SIGNATURES = {
     "dc_version": (C.c_int, []),
     "dc_device_count": (C.c_int, []),
     "dc_release_device": (C.c_int, [C.c_int]),
+    "dc_photon_set_depth_mode": (C.c_int, [C.c_int, C.c_int]),
+    "dc_photon_get_depth_mode": (C.c_int, [C.c_int, C.POINTER(C.c_int)]),
+    "dc_photon_depth_stats": (C.c_int, [C.c_int, C.POINTER(C.c_longlong)]),
     "dc_profile_enable": (C.c_int, [C.c_int, C.c_int]),
     "dc_profile_reset": (C.c_int, [C.c_int]),
     "dc_profile_read": (C.c_int, [C.c_int, C.c_int, C.POINTER(C.c_char_p), C.POINTER(C.c_int),
@@ -147,6 +155,8 @@ SIGNATURES = {
     "dc_photon_beam_probe_list": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_int), C.c_void_p,
                                             C.c_int]),
     "dc_photon_beam_probe": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
+    "dc_photon_beam_fluence_dose": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "dc_photon_beam_fluence_adjoint": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "dc_gamma": (C.c_int, [C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_int, _F3, C.c_void_p, C.c_void_p, C.c_longlong,
                            C.c_float, C.c_float, C.c_float, C.c_float, C.c_void_p, C.c_void_p]),
     "dc_net_packed_fragments": (C.c_longlong, [C.c_int, C.c_int, C.c_int]),

@@ -121,7 +121,8 @@ int dc_debug_bounds(int gpu_id, unsigned long long *violation, int *enabled) {
         DC_CUDA(cudaDeviceSynchronize());
         unsigned long long v = 0;
         for (unsigned long long w : {take_bounds_wet(), take_bounds_photon(), take_bounds_proton(),
-                                     take_bounds_basis(), take_bounds_noalloc()})
+                                     take_bounds_basis(), take_bounds_noalloc(), take_bounds_xray(),
+                                     take_bounds_fluence()})
             if (v == 0) v = w;
         *violation = v;
     });
@@ -154,6 +155,38 @@ int dc_device_count(void) {
 
 int dc_release_device(int gpu_id) {
     return guarded([&] { release_context(gpu_id); });
+}
+
+int dc_photon_set_depth_mode(int gpu_id, int mode) {
+    return guarded([&] {
+        need(mode == DC_DEPTH_MARCH || mode == DC_DEPTH_LATTICE, "depth mode must be 0 (march) or 1 (lattice).");
+        DeviceContext &ctx = context(gpu_id);
+        std::lock_guard<std::mutex> lk(ctx.mu);
+        ctx.photon_depth_mode = mode;
+    });
+}
+
+int dc_photon_get_depth_mode(int gpu_id, int *mode) {
+    return guarded([&] {
+        need(mode != nullptr, "'mode' must not be NULL.");
+        DeviceContext &ctx = context(gpu_id);
+        std::lock_guard<std::mutex> lk(ctx.mu);
+        *mode = ctx.photon_depth_mode;
+    });
+}
+
+int dc_photon_depth_stats(int gpu_id, long long *marched) {
+    return guarded([&] {
+        need(marched != nullptr, "'marched' must not be NULL.");
+        DeviceContext &ctx = context(gpu_id);
+        std::lock_guard<std::mutex> lk(ctx.mu);
+        *marched = -1;
+        if (ctx.xstat.ptr == nullptr) return;
+        DC_CUDA(cudaDeviceSynchronize());
+        unsigned v = 0;
+        DC_CUDA(cudaMemcpy(&v, ctx.xstat.ptr, sizeof(v), cudaMemcpyDeviceToHost));
+        *marched = v == 0xffffffffu ? -1 : (long long)v;
+    });
 }
 
 int dc_profile_enable(int gpu_id, int on) {

@@ -14,6 +14,28 @@ void launch_wet_march(DeviceContext &ctx, const Grid &g, const Frame &f, cudaTex
 void launch_wet_smooth(DeviceContext &ctx, const Grid &g, const Frame &f, const float *wet, float *wet_s,
                        cudaStream_t s);
 
+// ---- photon radiological depth on a ray lattice (dc_xray.cu) -------------
+// Rays from the source through (a0 + ia*pa, b0 + ib*pa) on the head frame's
+// isocentre plane; nodes at distances (m0 + m) mm from the source.
+struct XrayLattice {
+    float a0, b0, pa, inv_pa;
+    int na, nb, m0, nm;
+    float sad;         // source distance (mm)
+    float tau;         // largest spread of the four rays' sums interpolated (mm x density)
+    float3 src;        // source, image frame relative to the isocentre
+    float3 ex, ey, ez; // head-frame axes in the image frame
+};
+// Lattice geometry for this grid and beam; false when the lattice does not
+// apply (source inside or next to the volume, lattice too large).
+bool plan_xray_lattice(const Grid &g, const Frame &f, XrayLattice &L);
+// Photon WET (cm) of every voxel through the lattice, with the reference's
+// march for the voxels the lattice cannot serve (listed in list/n_list, which
+// need room for every voxel); the plain march when the lattice does not apply.
+// `stats` (device word, or null) receives the number of marched voxels
+// (0xffffffff when the lattice did not apply).
+void launch_xray_depth(DeviceContext &ctx, const Grid &g, const Frame &f, cudaTextureObject_t density, float *wet,
+                       int *list, unsigned *n_list, DeviceBuffer &lattice, unsigned *stats, cudaStream_t s);
+
 // ---- proton pencil beam (dc_proton.cu) -----------------------------------
 // One energy layer: a run of spots with the same energy id
 // (reference Layer, IMPTClasses.cuh:17-26; importLayers IMPTClasses.cu:37-67).
@@ -80,6 +102,8 @@ unsigned long long take_bounds_photon();
 unsigned long long take_bounds_proton();
 unsigned long long take_bounds_basis();
 unsigned long long take_bounds_noalloc();
+unsigned long long take_bounds_xray();
+unsigned long long take_bounds_fluence();
 
 // Builds the sorted spot table and the layer table on the host.  Throws
 // Error(DC_ERR_VALUE) for malformed input.

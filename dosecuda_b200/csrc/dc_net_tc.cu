@@ -19,7 +19,10 @@
 // them to an mbarrier, and every warp reads its 32 TMEM lanes back
 // (tcgen05.ld 32x32b.x16) for the bf16 store and the instance-norm sums.
 // The wait on the mbarrier is bounded: on expiry the kernel records an error
-// (dc_net_tc_error) and skips the epilogue instead of hanging.
+// (dc_net_tc_error) and skips the epilogue instead of hanging.  It then frees
+// its tensor memory although MMAs it issued may still be writing there, so a
+// recorded expiry outside the self-test (which issues none) leaves the
+// device's later results untrustworthy: callers treat it as a device error.
 //
 // Measured on B200: one tcgen05.mma of M=128, K=16 costs ~26 ns whatever N
 // up to 64, so with 16 output channels the tensor cores top out near

@@ -36,7 +36,11 @@ struct dc_photon_beam {
     float origin[3] = {0, 0, 0};
     VolumeArray density;
     VolumeArray td;
-    DeviceBuffer wet, electron, active, dirs, probe;
+    DeviceBuffer wet, electron, active, dirs, probe, xlat, td_lin;
+    // fluence mode: the unmodulated TERMA and electron term of the last
+    // dc_photon_beam_terma, and the adjoint's scratch
+    DeviceBuffer terma0, electron0, fl_h;
+    bool have_e0 = false;
     PhotonParams P{};
     CccsCones C{};
     Frame f{};
@@ -61,6 +65,9 @@ struct dc_photon_beam {
         w.dens_tex = density.texture(kAirDensity);
         w.td_surf = td.surf;
         w.td_tex = td.texture(0.0f, kAirDensity);
+        w.xlat = &xlat;
+        w.td_lin = &td_lin;
+        w.depth_mode = context(device).photon_depth_mode;
         return w;
     }
     ~dc_photon_beam() {
@@ -68,6 +75,11 @@ struct dc_photon_beam {
         density.release();
         td.release();
         wet.release();
+        xlat.release();
+        td_lin.release();
+        terma0.release();
+        electron0.release();
+        fl_h.release();
         electron.release();
         active.release();
         dirs.release();
@@ -347,8 +359,13 @@ int dc_photon_beam_terma(dc_photon_beam *b, const dc_photon_model *model, const 
         b->field[0] = x1, b->field[1] = x2, b->field[2] = y1, b->field[3] = y2;
         DC_CUDA(cudaSetDevice(b->device));
         DeviceContext &ctx = context(b->device);
-        enqueue_terma(ctx, b->g, b->f, b->P, b->C, b->work(), nullptr, terma_out_dev, as_stream(stream));
+        float *t0 = static_cast<float *>(b->terma0.ensure((size_t)b->g.n() * sizeof(float)));
+        enqueue_terma(ctx, b->g, b->f, b->P, b->C, b->work(), nullptr, t0, as_stream(stream));
+        if (terma_out_dev)
+            DC_CUDA(cudaMemcpyAsync(terma_out_dev, t0, (size_t)b->g.n() * sizeof(float), cudaMemcpyDeviceToDevice,
+                                    as_stream(stream)));
         b->have_terma = true;
+        b->have_e0 = false;
         // the probe of this control point, selected on the host while the
         // TERMA kernels run
         select_and_upload_probe(*b, as_stream(stream));
@@ -364,6 +381,73 @@ int dc_photon_beam_dose(dc_photon_beam *b, float *dose_out_dev, void *stream) {
         cudaStream_t s = as_stream(stream);
         DC_CUDA(cudaMemsetAsync(dose_out_dev, 0, (size_t)b->g.n() * sizeof(float), s));
         enqueue_cccs(ctx, b->g, b->f, b->C, b->work(), b->dose_scale, dose_out_dev, s);
+    });
+}
+
+namespace {
+
+FluenceMap fluence_map(const dc_photon_beam &b, const dc_fluence_map *m) {
+    need(m != nullptr, "fluence map must not be NULL.");
+    need(m->na >= 1 && m->nb >= 1 && (long long)m->na * m->nb <= (1LL << 24), "fluence map size out of range.");
+    need(std::isfinite(m->a0) && std::isfinite(m->b0) && std::isfinite(m->pitch) && m->pitch > 0.0f,
+         "fluence map origin and pitch must be finite, the pitch positive.");
+    FluenceMap M{};
+    M.na = m->na;
+    M.nb = m->nb;
+    M.a0 = m->a0;
+    M.b0 = m->b0;
+    M.inv_pitch = 1.0f / m->pitch;
+    M.sad = b.src_dist;
+    return M;
+}
+
+// E0: the electron term of the last TERMA pass, kept before a fluence
+// forward overwrites the work set's electron volume.
+const float *electron0(dc_photon_beam &b, cudaStream_t s) {
+    const size_t bytes = (size_t)b.g.n() * sizeof(float);
+    float *e0 = static_cast<float *>(b.electron0.ensure(bytes));
+    if (!b.have_e0) {
+        DC_CUDA(cudaMemcpyAsync(e0, b.electron.ptr, bytes, cudaMemcpyDeviceToDevice, s));
+        b.have_e0 = true;
+    }
+    return e0;
+}
+
+}  // namespace
+
+int dc_photon_beam_fluence_dose(dc_photon_beam *b, const dc_fluence_map *map, const float *fluence_dev,
+                                float *dose_out_dev, void *stream) {
+    return guarded([&] {
+        need(b != nullptr && fluence_dev != nullptr && dose_out_dev != nullptr,
+             "beam, fluence and output must not be NULL.");
+        need(b->have_terma, "dc_photon_beam_terma must run first.");
+        const FluenceMap M = fluence_map(*b, map);
+        DC_CUDA(cudaSetDevice(b->device));
+        DeviceContext &ctx = context(b->device);
+        cudaStream_t s = as_stream(stream);
+        const PhotonWork w = b->work();
+        const float *e0 = electron0(*b, s);
+        enqueue_fluence_modulate(ctx, b->g, b->f, M, fluence_dev, b->terma0.as<float>(), e0, w, s);
+        DC_CUDA(cudaMemsetAsync(dose_out_dev, 0, (size_t)b->g.n() * sizeof(float), s));
+        enqueue_cccs(ctx, b->g, b->f, b->C, w, b->dose_scale, dose_out_dev, s);
+    });
+}
+
+int dc_photon_beam_fluence_adjoint(dc_photon_beam *b, const dc_fluence_map *map, const float *grad_dose_dev,
+                                   double *grad_fluence_dev, void *stream) {
+    return guarded([&] {
+        need(b != nullptr && grad_dose_dev != nullptr && grad_fluence_dev != nullptr,
+             "beam, gradient and output must not be NULL.");
+        need(b->have_terma, "dc_photon_beam_terma must run first.");
+        const FluenceMap M = fluence_map(*b, map);
+        DC_CUDA(cudaSetDevice(b->device));
+        DeviceContext &ctx = context(b->device);
+        cudaStream_t s = as_stream(stream);
+        const PhotonWork w = b->work();
+        const float *e0 = electron0(*b, s);
+        float *h = static_cast<float *>(b->fl_h.ensure((size_t)b->g.n() * sizeof(float)));
+        enqueue_fluence_adjoint(ctx, b->g, b->f, b->C, M, b->dose_scale, b->terma0.as<float>(), e0, w, grad_dose_dev,
+                                h, grad_fluence_dev, s);
     });
 }
 

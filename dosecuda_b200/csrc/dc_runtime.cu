@@ -216,6 +216,9 @@ void DeviceContext::release_all() {
     vol_c.release();
     electron.release();
     active.release();
+    xlat.release();
+    xstat.release();
+    td_lin.release();
     small.release();
     lut.release();
     tables.release();

@@ -109,6 +109,32 @@ def photon_dose(density: torch.Tensor, grid, model, cp, out=None, stream=None, v
     return out
 
 
+PHOTON_DEPTH_MODES = {"march": 0, "lattice": 1}
+
+
+def photon_depth_mode(gpu_id: int = 0, mode: str | None = None) -> str:
+    """Select how photon calls on ``gpu_id`` compute the radiological depth
+    ("march": the reference's per-voxel 1 mm march, the default; "lattice":
+    the beam's-eye-view ray lattice with the march as its fallback) and
+    return the mode in force."""
+    lib = _lib.load()
+    if mode is not None:
+        if mode not in PHOTON_DEPTH_MODES:
+            raise ValueError("photon depth mode must be one of %s" % sorted(PHOTON_DEPTH_MODES))
+        _lib.raise_for(lib.dc_photon_set_depth_mode(gpu_id, PHOTON_DEPTH_MODES[mode]))
+    cur = C.c_int(-1)
+    _lib.raise_for(lib.dc_photon_get_depth_mode(gpu_id, C.byref(cur)))
+    return {v: k for k, v in PHOTON_DEPTH_MODES.items()}[cur.value]
+
+
+def photon_depth_marched(gpu_id: int = 0) -> int:
+    """Voxels the last lattice depth pass on ``gpu_id`` marched exactly (-1:
+    the last pass marched every voxel, or none ran).  Synchronises."""
+    v = C.c_longlong(0)
+    _lib.raise_for(_lib.load().dc_photon_depth_stats(gpu_id, C.byref(v)))
+    return int(v.value)
+
+
 def profile(gpu_id: int = 0, enable: bool | None = None, reset: bool = False):
     """Kernel timing control: enable/disable/reset, and read {kernel: (launches, ms)}."""
     lib = _lib.load()
@@ -372,6 +398,38 @@ class ProtonBatch:
         self.beam_spots.append(sp)
         return bid.value
 
+    def add_impt_plan(self, dose_grid, plan, rlsp: torch.Tensor | None = None) -> int:
+        """Add a whole IMPTPlan (for instance one read by
+        ``IMPTPlan.readPlanDicom``) on its IMPTDoseGrid: the grid's RLSP
+        (``RLSPFromHU`` of the plan's machine unless given) and every beam.
+        Beams are matched to beam models by range-shifter label as
+        ``computeIMPTPlan`` does (plan_impt.py:124-160); all must use this
+        batch's model.  The plan's dose is ``self.doses[pid]`` per fraction;
+        ``plan_dose(pid)`` applies ``n_fractions`` as computeIMPTPlan does."""
+        labels = list(np.asarray(plan.dicom_rangeshifter_label).astype(str))
+        for beam in plan.beam_list:
+            if str(beam.dicom_rangeshifter_label) not in labels:
+                raise ValueError("Beam model not found for rangeshifter ID %s" % beam.dicom_rangeshifter_label)
+            m = plan.beam_models[labels.index(str(beam.dicom_rangeshifter_label))]
+            if not (np.array_equal(np.asarray(m.divergence_params), np.asarray(self.model.divergence_params)) and
+                    np.array_equal(np.asarray(m.lut_idds), np.asarray(self.model.lut_idds))):
+                raise ValueError("beam with range shifter %s needs another beam model than this batch's"
+                                 % beam.dicom_rangeshifter_label)
+        if rlsp is None:
+            rlsp = torch.from_numpy(np.ascontiguousarray(dose_grid.RLSPFromHU(plan.machine_name),
+                                                         dtype=np.float32)).to(self.device)
+        pid = self.add_plan(dose_grid, rlsp)
+        for beam in plan.beam_list:
+            self.add_beam(pid, beam)
+        if not hasattr(self, "n_fractions"):
+            self.n_fractions = {}
+        self.n_fractions[pid] = float(plan.n_fractions)
+        return pid
+
+    def plan_dose(self, pid: int) -> torch.Tensor:
+        """Dose of plan ``pid`` over all fractions (the last ``dose()``)."""
+        return self.doses[pid] * getattr(self, "n_fractions", {}).get(pid, 1.0)
+
     def commit(self):
         lib = _lib.load()
         _lib.raise_for(lib.dc_proton_batch_commit(self._h))
@@ -550,6 +608,96 @@ class PhotonBeam:
         _lib.raise_for(_lib.load().dc_photon_beam_probe(self._h, vp, n, C.c_void_p(out.data_ptr()),
                                                          self._s(stream)))
         return out
+
+
+class PhotonFluenceBeam:
+    """One photon control point on the device with a beamlet fluence map:
+    the dose as a linear function of the map and its adjoint (C ABI
+    ``dc_photon_beam_fluence_dose`` / ``_adjoint``).
+
+    The map is a grid of beamlets on the beam's-eye-view isocentre plane
+    (head frame, mm): beamlet (ia, ib) sits at (a0 + ia*pitch, b0 + ib*pitch)
+    and values are a float32 tensor of shape (nb, na).  Each voxel's TERMA and
+    electron term are scaled by the map's bilinear interpolation at the
+    voxel's ray, so ``dose(ones)`` is the control point's CCCS dose (bit for
+    bit) and ``dose`` is linear in the map; ``adjoint(g)`` is the exact
+    gradient d(sum g D)/d map in float64 through the transpose of the
+    collapsed-cone superposition.  ``photon_fluence_dose_autograd`` wraps both
+    in a torch.autograd.Function.  ``field_map`` builds a map covering the
+    control point's open MLC field."""
+
+    def __init__(self, density: torch.Tensor, grid, model, cp, na: int, nb: int, a0: float, b0: float,
+                 pitch: float, views=None):
+        self.beam = PhotonBeam(grid, density.shape, device=density.device)
+        self.beam.set_density(density)
+        self.beam.terma(model, cp, views=views)
+        self.device = density.device
+        self.shape = tuple(density.shape)
+        self.map = _lib.FluenceMap(int(na), int(nb), float(a0), float(b0), float(pitch))
+        self.na, self.nb = int(na), int(nb)
+
+    @classmethod
+    def field_map(cls, density, grid, model, cp, pitch: float = 5.0, margin: float = 10.0, views=None):
+        """A map of ``pitch`` mm beamlets over the control point's open MLC
+        field (leaf pairs with x2 > x1, projected to the isocentre plane by the
+        leaves' own coordinates) plus ``margin`` mm on every side."""
+        mlc = np.asarray(cp.mlc, np.float32)
+        openp = mlc[:, 1] > mlc[:, 0]
+        if not openp.any():
+            raise ValueError("the control point has no open leaf pair")
+        a_lo, a_hi = float(mlc[openp, 0].min()) - margin, float(mlc[openp, 1].max()) + margin
+        yb = mlc[openp, 2] - 0.5 * mlc[openp, 3]
+        yt = mlc[openp, 2] + 0.5 * mlc[openp, 3]
+        b_lo, b_hi = float(yb.min()) - margin, float(yt.max()) + margin
+        na = int(np.ceil((a_hi - a_lo) / pitch)) + 1
+        nb = int(np.ceil((b_hi - b_lo) / pitch)) + 1
+        return cls(density, grid, model, cp, na, nb, a_lo, b_lo, pitch, views=views)
+
+    def _check_map(self, t: torch.Tensor, dtype):
+        if tuple(t.shape) != (self.nb, self.na) or t.dtype != dtype or t.device != self.device or \
+                not t.is_contiguous():
+            raise ValueError("fluence must be a contiguous %s tensor of shape (%d, %d) on %s"
+                             % (dtype, self.nb, self.na, self.device))
+
+    def dose(self, fluence: torch.Tensor, out: torch.Tensor | None = None, stream=None) -> torch.Tensor:
+        f = fluence.detach().to(device=self.device, dtype=torch.float32).contiguous()
+        self._check_map(f, torch.float32)
+        out = torch.empty(self.shape, dtype=torch.float32, device=self.device) if out is None else out
+        _check_volume(out, "out")
+        _lib.raise_for(_lib.load().dc_photon_beam_fluence_dose(self.beam._h, C.byref(self.map),
+                                                                C.c_void_p(f.data_ptr()), C.c_void_p(out.data_ptr()),
+                                                                self.beam._s(stream)))
+        return out
+
+    def adjoint(self, grad_dose: torch.Tensor, stream=None) -> torch.Tensor:
+        g = grad_dose.detach().to(device=self.device, dtype=torch.float32).contiguous()
+        if tuple(g.shape) != self.shape:
+            raise ValueError("grad_dose must have the volume's shape")
+        out = torch.empty((self.nb, self.na), dtype=torch.float64, device=self.device)
+        _lib.raise_for(_lib.load().dc_photon_beam_fluence_adjoint(self.beam._h, C.byref(self.map),
+                                                                   C.c_void_p(g.data_ptr()),
+                                                                   C.c_void_p(out.data_ptr()), self.beam._s(stream)))
+        return out
+
+    def close(self):
+        self.beam.close()
+
+
+class _PhotonFluenceFn(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, fluence, beam):
+        ctx.beam = beam
+        return beam.dose(fluence)
+
+    @staticmethod
+    def backward(ctx, grad):
+        return ctx.beam.adjoint(grad).to(torch.float32), None
+
+
+def photon_fluence_dose_autograd(fluence: torch.Tensor, beam: PhotonFluenceBeam) -> torch.Tensor:
+    """Differentiable photon dose in the beamlet fluence map: forward is the
+    modulated TERMA + CCCS, backward the hand-written CCCS transpose."""
+    return _PhotonFluenceFn.apply(fluence, beam)
 
 
 def gamma_counts(eval_dose: torch.Tensor, spacing, ref: torch.Tensor, voxels: torch.Tensor | int | None = None,

@@ -147,6 +147,28 @@ int dc_device_count(void);
 /* Free the cached device buffers, textures and streams held for gpu_id. */
 int dc_release_device(int gpu_id);
 
+/* No counterpart in the reference (its ray trace, CudaClasses.cu:180-228,
+ * is the only mode).  How photon calls on gpu_id compute the radiological
+ * depth that TERMA attenuates with:
+ *   DC_DEPTH_MARCH   (0): the default: the reference's per-voxel 1 mm
+ *                         march, sample for sample;
+ *   DC_DEPTH_LATTICE (1): the density integrated once along a
+ *                         beam's-eye-view lattice of rays from the source and
+ *                         interpolated per voxel, with the reference's exact
+ *                         sample count, its boundary samples fetched exactly,
+ *                         and the exact march wherever neighbouring lattice
+ *                         rays disagree by more than 0.03 cm of WET.
+ * Applies to calls enqueued after it returns; proton WET always uses the
+ * march. */
+#define DC_DEPTH_MARCH 0
+#define DC_DEPTH_LATTICE 1
+int dc_photon_set_depth_mode(int gpu_id, int mode);
+int dc_photon_get_depth_mode(int gpu_id, int *mode);
+/* Voxels the last lattice depth pass of a photon call on gpu_id marched
+ * exactly (its fallback); -1 when the last pass marched every voxel or none
+ * ran.  Synchronises the device. */
+int dc_photon_depth_stats(int gpu_id, long long *marched);
+
 /* Kernel timing: when enabled, every kernel the library launches is
  * bracketed by CUDA events on its own stream.  dc_profile_read synchronises
  * the device and returns, per kernel name, the launch count and the summed
@@ -405,6 +427,26 @@ int dc_photon_beam_probe_list(const dc_photon_beam *beam, const int **voxels_dev
 /* CCCS dose at n listed voxels (voxels_dev NULL: the selected list). */
 int dc_photon_beam_probe(dc_photon_beam *beam, const int *voxels_dev, int n, float *dose_out_dev, void *stream);
 
+/* No counterpart in the reference (its TERMA has no fluence input,
+ * IMRTClasses.cu:209-250).  A beamlet fluence map on the beam's-eye-view
+ * isocentre plane (head frame: a along x, b along y, mm): beamlet (ia, ib)
+ * at (a0 + ia*pitch, b0 + ib*pitch), values row-major [nb][na].  Each voxel's
+ * TERMA and electron term of the last dc_photon_beam_terma are scaled by the
+ * map's bilinear interpolation at the voxel's ray (clamped to the map's
+ * edge), with the CCCS mask of the unmodulated TERMA, so the dose is linear
+ * in the fluence; an all-ones map gives dc_photon_beam_dose bit for bit.
+ * fluence_dose leaves the modulated TERMA in the beam (dose/probe then use
+ * it); fluence_adjoint writes d(sum_v grad_dose_v D_v)/d fluence (float64,
+ * one per beamlet), the transpose of the collapsed-cone superposition. */
+typedef struct dc_fluence_map {
+    int na, nb;
+    float a0, b0, pitch;
+} dc_fluence_map;
+int dc_photon_beam_fluence_dose(dc_photon_beam *beam, const dc_fluence_map *map, const float *fluence_dev,
+                                float *dose_out_dev, void *stream);
+int dc_photon_beam_fluence_adjoint(dc_photon_beam *beam, const dc_fluence_map *map, const float *grad_dose_dev,
+                                   double *grad_fluence_dev, void *stream);
+
 /* Gamma index of the evaluated volume eval (nz,ny,nx) against reference
  * doses: ref[i] at voxel voxels[i] (i < n), or, with voxels NULL, the
  * reference volume ref.  Global dose criterion dd_frac*dose_norm (dose_norm
@@ -493,7 +535,11 @@ int dc_net_conv_tc(int gpu_id, const void *x_dev, int n, int d, int h, int w, in
                    long long wtc_bytes, int cout, void *y_dev, double *stats_dev, void *stream);
 /* Reads and clears the flag the tensor-core convolution sets when its
  * bounded wait for the tensor cores expired (that launch's output is not
- * written).  Synchronous. */
+ * written).  When it is set by a launch whose MMAs were issued (anything but
+ * dc_net_tc_selftest, which withholds them), the expired CTA has released
+ * tensor memory that those MMAs may still write, so every later result on
+ * that device is suspect until the process recreates its CUDA context;
+ * treat a set flag as a device error.  Synchronous. */
 int dc_net_tc_error(int gpu_id, int *flag);
 /* Failure self-test of that bounded wait: runs one tile with its MMAs
  * withheld, so the wait must expire; *wait_expired = 1 when the kernel

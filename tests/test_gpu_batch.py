@@ -100,3 +100,44 @@ def test_weights_and_cuda_graph_replay(batch):
         for d, r in zip(b.doses, d1):
             assert dose_diff(d.cpu().numpy(), 2.0 * r.cpu().numpy()) <= 1e-5
     del g
+
+
+def test_dicom_plan_feeds_the_batch(monkeypatch):
+    """An RT Ion plan read by IMPTPlan.readPlanDicom (synthetic dataset through
+    a stand-in pydicom, as in test_dicom_readers.py) goes into the batched
+    engine whole (ProtonBatch.add_impt_plan) and gives computeIMPTPlan's dose."""
+    torch = pytest.importorskip("torch")
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from types import SimpleNamespace as NS
+    from dosecuda_b200 import engine, phantoms, plan_impt
+    from test_dicom_readers import _fake_pydicom
+    plan = plan_impt.IMPTPlan()
+    labels = plan.beam_models[0].energy_table["energy_label"].to_numpy()
+    rng = np.random.default_rng(7)
+    beams = []
+    for ga, ta in ((0.0, 0.0), (70.0, 10.0)):
+        cps = []
+        for e in labels[[12, 16, 20]]:
+            pos = rng.uniform(-15, 15, size=(6, 2)).round(1).ravel().tolist()
+            cp = NS(NominalBeamEnergy=float(e), ScanSpotPositionMap=pos,
+                    ScanSpotMetersetWeights=rng.uniform(0.2, 1.5, 6).round(3).tolist(), GantryAngle=ga,
+                    PatientSupportAngle=ta, IsocenterPosition=[2.0, -1.0, 0.5])
+            cps += [cp, NS(NominalBeamEnergy=float(e), ScanSpotPositionMap=pos, ScanSpotMetersetWeights=[0.0] * 6)]
+        beams.append(NS(NumberOfRangeShifters=0, IonControlPointSequence=cps, RangeShifterSequence=[]))
+    ds = NS(FractionGroupSequence=[NS(NumberOfFractionsPlanned=3)], IonBeamSequence=beams)
+    fake = _fake_pydicom({"ion.dcm": ds})
+    monkeypatch.setattr(plan_impt, "_pydicom", lambda: fake)
+    plan.readPlanDicom("ion.dcm")
+    grid = phantoms.proton_phantom((40, 44, 36), 3.0, seed=3)
+    b = engine.ProtonBatch(plan.beam_models[0])
+    pid = b.add_impt_plan(grid, plan)
+    b.commit()
+    b.wet()
+    b.dose()
+    torch.cuda.synchronize()
+    grid.computeIMPTPlan(plan)
+    got = b.plan_dose(pid).cpu().numpy()
+    assert grid.dose.max() > 0
+    assert dose_diff(got, grid.dose) <= 1e-5
+    b.close()

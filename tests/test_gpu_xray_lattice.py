@@ -1,0 +1,138 @@
+"""Photon radiological depth on the beam's-eye-view ray lattice (depth mode
+"lattice", csrc/dc_xray.cu) against the reference's per-voxel march (depth
+mode "march", sample for sample rayTraceKernel, CudaClasses.cu:180-228), and
+the photon dose it gives against the reference's own build and the FP64
+oracle.
+
+The lattice interpolates each voxel's density integral from the four lattice
+rays around its ray and marches exactly wherever they disagree by more than
+0.3 mm of unit density (0.03 cm of WET), so TERMA may move by at most the
+attenuation of 0.03 cm of water; the dose is held to the parity bar."""
+import glob
+import os
+import sys
+
+import numpy as np
+import pytest
+
+from conftest import ROOT
+from dosecheck import dose_diff, gamma_pass_rate
+
+pytestmark = pytest.mark.gpu
+
+GEOMETRIES = {
+    # name: (phantom kwargs, plan kwargs)
+    "small_photon_128": ({}, {}),
+    "gantry30_coll20": ({"shape": (96, 96, 96), "spacing": 3.0, "seed": 4}, {"gantry": 30.0, "collimator": 20.0,
+                                                                             "field_cm": (8.0, 12.0)}),
+    "gantry250_couch30": ({"shape": (80, 96, 72), "spacing": 3.5, "seed": 5}, {"gantry": 250.0, "couch": 30.0,
+                                                                               "field_cm": (6.0, 6.0)}),
+    "odd_small": ({"shape": (37, 41, 29), "spacing": 4.0, "seed": 6, "lung_mm": (30.0, 24.0, 20.0),
+                   "bone_mm": 12.0}, {"gantry": 45.0, "field_cm": (6.0, 10.0)}),
+}
+
+
+@pytest.fixture(scope="module")
+def engine():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from dosecuda_b200 import engine as eng
+    saved = eng.photon_depth_mode(0)
+    yield eng
+    eng.photon_depth_mode(0, saved)
+
+
+def _case(name):
+    from dosecuda_b200 import phantoms
+    pk, bk = GEOMETRIES[name]
+    grid, plan = phantoms.photon_small(**pk, **bk)
+    model, cp = plan.beam_models[0], plan.beam_list[0].cp_list[0]
+    return grid, plan, model, cp, grid.DensityFromHU(plan.machine_name)
+
+
+def _terma(engine, mode, grid, model, cp, density):
+    import torch
+    engine.photon_depth_mode(0, mode)
+    beam = engine.PhotonBeam(grid, density.shape)
+    beam.set_density(torch.from_numpy(density).cuda())
+    t = beam.terma(model, cp, out=True)
+    torch.cuda.synchronize()
+    out = t.cpu().numpy().astype(np.float64)
+    beam.close()
+    return out
+
+
+def _dose(engine, mode, grid, model, cp, density):
+    from dosecuda_b200 import dose_kernels, phantoms
+    engine.photon_depth_mode(0, mode)
+    d = dose_kernels.photon_dose_cuda(model, phantoms.volume_object(grid, density), cp, 0)
+    marched = engine.photon_depth_marched(0)
+    return d, marched
+
+
+@pytest.mark.parametrize("name", sorted(GEOMETRIES))
+def test_lattice_terma_within_attenuation_of_its_tolerance(engine, name):
+    grid, plan, model, cp, density = _case(name)
+    t_m = _terma(engine, "march", grid, model, cp, density)
+    t_l = _terma(engine, "lattice", grid, model, cp, density)
+    mask = t_m > 1e-3 * t_m.max()
+    rel = np.abs(t_l - t_m)[mask] / t_m[mask]
+    # 0.03 cm of WET at the spectrum's largest attenuation coefficient, with the
+    # off-axis softening factor's largest value
+    mu_max = float(np.max(model.spectrum_attenuation_coefficients)) * float(np.max(model.profile_softening))
+    bound = float(np.expm1(mu_max * 0.03))
+    print("\n%s: TERMA rel. diff max %.2e mean %.2e (bound %.2e)" % (name, rel.max(), rel.mean(), bound))
+    assert rel.max() <= bound
+    assert rel.mean() <= 0.1 * bound
+
+
+@pytest.mark.parametrize("name", sorted(GEOMETRIES))
+def test_lattice_dose_matches_march_and_oracle(engine, name):
+    import oracle
+    grid, plan, model, cp, density = _case(name)
+    d_m, _ = _dose(engine, "march", grid, model, cp, density)
+    d_l, marched = _dose(engine, "lattice", grid, model, cp, density)
+    sp = float(grid.spacing[0])
+    o, _ = oracle.photon_dose(density, np.float32([sp, sp, sp]), grid.origin, model, cp.iso, cp.mu, cp.ga, cp.ca,
+                              cp.ta, np.ascontiguousarray(cp.mlc))
+    dd_m = dose_diff(d_l, d_m)
+    print("\n%s: lattice vs march |dD| %.5f Dmax; vs oracle %.5f; voxels marched %d of %d (%.2f %%)"
+          % (name, dd_m, dose_diff(d_l, o), marched, density.size, 100.0 * max(marched, 0) / density.size))
+    assert marched >= 0  # the lattice ran
+    assert dd_m <= 0.002
+    assert gamma_pass_rate(d_l, d_m, sp) >= 0.999
+    assert dose_diff(d_l, o) <= 0.005
+    assert gamma_pass_rate(d_l, o, sp) >= 0.995
+
+
+def test_lattice_dose_vs_reference_build_whole_volume(engine):
+    """The 128^3 workload with the isocentre half a voxel off the grid (where
+    the reference's TERMA is sound, test_gpu_reference_terma.py): the engine
+    in lattice mode against the reference's build on every voxel."""
+    ref_dir = os.path.join(ROOT, "oracle", "_ref")
+    if not glob.glob(os.path.join(ref_dir, "dose_kernels*.so")):
+        pytest.skip("reference build oracle/_ref not present")
+    sys.path.insert(0, ref_dir)
+    import dose_kernels as ref
+    sys.path.remove(ref_dir)
+    from dosecuda_b200 import phantoms
+    grid, plan, model, cp, density = _case("small_photon_128")
+    cp.iso = np.array(cp.iso, np.float32) + np.float32([0.5 * grid.spacing[0], 0.0, 0.0])
+    vol = phantoms.volume_object(grid, density)
+    engine.photon_depth_mode(0, "lattice")
+    from dosecuda_b200 import dose_kernels as dk
+    d = dk.photon_dose_cuda(model, vol, cp, 0)
+    r = ref.photon_dose_cuda(model, vol, cp, 0)
+    dd, g = dose_diff(d, r), gamma_pass_rate(d, r, float(grid.spacing[0]))
+    print("\nlattice engine vs reference build: |dD| %.5f Dmax, gamma %.5f" % (dd, g))
+    assert dd <= 0.005
+    assert g >= 0.995
+
+
+def test_depth_mode_is_validated_and_reported(engine):
+    assert engine.photon_depth_mode(0) in ("lattice", "march")
+    with pytest.raises(ValueError):
+        engine.photon_depth_mode(0, "siddon")
+    assert engine.photon_depth_mode(0, "march") == "march"
+    assert engine.photon_depth_mode(0, "lattice") == "lattice"
