@@ -155,6 +155,7 @@ SIGNATURES = {
     "dc_photon_beam_probe_list": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_int), C.c_void_p,
                                             C.c_int]),
     "dc_photon_beam_probe": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
+    "dc_photon_beam_dose_sweep": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     "dc_photon_beam_fluence_dose": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "dc_photon_beam_fluence_adjoint": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "dc_gamma": (C.c_int, [C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_int, _F3, C.c_void_p, C.c_void_p, C.c_longlong,

@@ -122,7 +122,7 @@ int dc_debug_bounds(int gpu_id, unsigned long long *violation, int *enabled) {
         unsigned long long v = 0;
         for (unsigned long long w : {take_bounds_wet(), take_bounds_photon(), take_bounds_proton(),
                                      take_bounds_basis(), take_bounds_noalloc(), take_bounds_xray(),
-                                     take_bounds_fluence()})
+                                     take_bounds_fluence(), take_bounds_sweep()})
             if (v == 0) v = w;
         *violation = v;
     });

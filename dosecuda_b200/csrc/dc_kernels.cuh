@@ -104,6 +104,7 @@ unsigned long long take_bounds_basis();
 unsigned long long take_bounds_noalloc();
 unsigned long long take_bounds_xray();
 unsigned long long take_bounds_fluence();
+unsigned long long take_bounds_sweep();
 
 // Builds the sorted spot table and the layer table on the host.  Throws
 // Error(DC_ERR_VALUE) for malformed input.

@@ -135,6 +135,14 @@ void enqueue_fluence_adjoint(DeviceContext &ctx, const Grid &g, const Frame &f, 
                              const FluenceMap &M, float dose_scale, const float *T0, const float *E0,
                              const PhotonWork &w, const float *grad_dose, float *h, double *grad_F, cudaStream_t s);
 
+// The CCCS by cone-direction sweeps over line lattices (dc_cccs_sweep.cu):
+// an approximation of enqueue_cccs (no per-voxel kernel tilt, windows
+// interpolated between lattice lines).  Synchronises the stream once (the
+// active voxels' bounding box sizes the lattices).
+void enqueue_cccs_sweep(DeviceContext &ctx, const Grid &g, const Frame &f, const CccsCones &C, const PhotonWork &w,
+                        float dose_scale, float *dose_dev, DeviceBuffer &lattice, DeviceBuffer &acc_buf,
+                        DeviceBuffer &box_buf, cudaStream_t s);
+
 // Enqueues ray trace -> TERMA -> CCCS for one control point on stream s.
 // The density volume must already be in ctx.density; dose_dev: device output.
 void run_photon_pipeline(DeviceContext &ctx, const Grid &g, const Frame &f, const PhotonParams &P,

@@ -40,6 +40,7 @@ struct dc_photon_beam {
     // fluence mode: the unmodulated TERMA and electron term of the last
     // dc_photon_beam_terma, and the adjoint's scratch
     DeviceBuffer terma0, electron0, fl_h;
+    DeviceBuffer sweep_lat, sweep_acc, sweep_box;  // cone-direction sweep mode
     bool have_e0 = false;
     PhotonParams P{};
     CccsCones C{};
@@ -80,6 +81,9 @@ struct dc_photon_beam {
         terma0.release();
         electron0.release();
         fl_h.release();
+        sweep_lat.release();
+        sweep_acc.release();
+        sweep_box.release();
         electron.release();
         active.release();
         dirs.release();
@@ -448,6 +452,20 @@ int dc_photon_beam_fluence_adjoint(dc_photon_beam *b, const dc_fluence_map *map,
         float *h = static_cast<float *>(b->fl_h.ensure((size_t)b->g.n() * sizeof(float)));
         enqueue_fluence_adjoint(ctx, b->g, b->f, b->C, M, b->dose_scale, b->terma0.as<float>(), e0, w, grad_dose_dev,
                                 h, grad_fluence_dev, s);
+    });
+}
+
+int dc_photon_beam_dose_sweep(dc_photon_beam *b, float *dose_out_dev, void *stream) {
+    return guarded([&] {
+        need(b != nullptr && dose_out_dev != nullptr, "beam and output must not be NULL.");
+        need(b->have_terma, "dc_photon_beam_terma must run first.");
+        need(b->g.sx == b->g.sy && b->g.sx == b->g.sz, "the sweep needs isotropic voxels.");
+        DC_CUDA(cudaSetDevice(b->device));
+        DeviceContext &ctx = context(b->device);
+        cudaStream_t s = as_stream(stream);
+        DC_CUDA(cudaMemsetAsync(dose_out_dev, 0, (size_t)b->g.n() * sizeof(float), s));
+        enqueue_cccs_sweep(ctx, b->g, b->f, b->C, b->work(), b->dose_scale, dose_out_dev, b->sweep_lat, b->sweep_acc,
+                           b->sweep_box, s);
     });
 }
 

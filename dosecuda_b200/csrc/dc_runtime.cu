@@ -185,6 +185,12 @@ void VolumeArray::release() {
 
 // ---------------------------------------------------------------------------
 DeviceContext::DeviceContext(int dev) : device(dev) {
+    // DC_PHOTON_DEPTH=march|lattice sets the photon depth mode new contexts
+    // start with (dc_photon_set_depth_mode changes it afterwards)
+    if (const char *e = std::getenv("DC_PHOTON_DEPTH")) {
+        if (std::strcmp(e, "lattice") == 0) photon_depth_mode = 1;
+        if (std::strcmp(e, "march") == 0) photon_depth_mode = 0;
+    }
     DC_CUDA(cudaSetDevice(dev));
     DC_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
     for (auto &e : pin_ev) DC_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));

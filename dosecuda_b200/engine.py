@@ -580,6 +580,15 @@ class PhotonBeam:
         _lib.raise_for(_lib.load().dc_photon_beam_dose(self._h, C.c_void_p(out.data_ptr()), self._s(stream)))
         return out
 
+    def dose_sweep(self, out=None, stream=None) -> torch.Tensor:
+        """The CCCS by cone-direction sweeps over line lattices: an
+        approximation of ``dose`` (no per-voxel kernel tilt, windows
+        interpolated between lattice lines); synchronises once."""
+        if out is None:
+            out = torch.empty(self.shape, dtype=torch.float32, device=self.device)
+        _lib.raise_for(_lib.load().dc_photon_beam_dose_sweep(self._h, C.c_void_p(out.data_ptr()), self._s(stream)))
+        return out
+
     def select_probe(self, stream=None) -> int:
         n = C.c_int()
         _lib.raise_for(_lib.load().dc_photon_beam_probe_select(self._h, C.byref(n), self._s(stream)))

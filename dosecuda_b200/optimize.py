@@ -20,6 +20,9 @@ behind ``torch.autograd`` (``engine.proton_dose_autograd``).
   and target plus organs at risk are a small part of the grid.
 * ``ImrtOptimizer``: the same loop on the segment (control-point) weights of
   photon beams, through ``engine.PhotonPlanBasis`` and its adjoint kernel.
+* ``FluenceOptimizer``: the same loop on beamlet fluence maps of photon
+  control points, through ``engine.PhotonFluenceBeam`` (TERMA modulated by
+  the map, CCCS forward, the hand-written CCCS transpose backward).
 * ``save_influence_csr``/``load_influence_csr``: a dose-influence matrix
   (``ProtonBeamPlan.influence_csr``) cached as ``.npz``."""
 from __future__ import annotations
@@ -280,6 +283,57 @@ class ImrtOptimizer(ImptOptimizer):
 
     def dose_list(self, mu=None):
         raise NotImplementedError("segment weights are optimised on the full volume")
+
+
+class FluenceOptimizer(ImptOptimizer):
+    """Projected Adam on the beamlet fluence maps of photon control points.
+
+    ``beams``: one ``engine.PhotonFluenceBeam`` per control point (its TERMA
+    computed once); ``output_factors`` (default 1) scale each control point's
+    dose as the plan loop does (plan_imrt.py:151-153).  The plan dose for maps
+    F is sum_b OF_b D_b(F_b), differentiable through
+    ``engine.photon_fluence_dose_autograd`` (modulated TERMA + CCCS forward,
+    the CCCS transpose backward); F = 1 is the plan as delivered.  Maps are
+    kept >= 0 after every step.  The loop, the objective, ``scale_to``,
+    checkpoint and resume are ``ImptOptimizer``'s."""
+
+    def __init__(self, beams, objective: DoseObjective, output_factors=None, fluence: torch.Tensor | None = None,
+                 lr: float | None = None, lr_frac: float = 0.02):
+        self.plans = list(beams)
+        if not self.plans:
+            raise ValueError("at least one control point is required")
+        self.wets = [None] * len(self.plans)
+        self.objective = objective
+        self.sizes = [int(b.na * b.nb) for b in self.plans]
+        of = [1.0] * len(self.plans) if output_factors is None else [float(x) for x in output_factors]
+        if len(of) != len(self.plans):
+            raise ValueError("one output factor per control point is required")
+        self.output_factors = of
+        dev = self.plans[0].device
+        f0 = torch.ones(sum(self.sizes), dtype=torch.float32, device=dev) if fluence is None else fluence
+        if f0.numel() != sum(self.sizes):
+            raise ValueError("fluence must hold one value per beamlet of all control points")
+        self.mu = f0.detach().to(device=dev, dtype=torch.float32).clone().requires_grad_(True)
+        self.lr = float(lr) if lr is not None else float(lr_frac * self.mu.detach().mean().item())
+        self.opt = torch.optim.Adam([self.mu], lr=self.lr)
+        self.iteration = 0
+        self.value = None
+        self.voxels = "volume"
+        self._list = None
+
+    def dose(self, mu: torch.Tensor | None = None) -> torch.Tensor:
+        """Plan dose for fluence maps ``mu`` (default: the current maps, all
+        control points' beamlets concatenated); differentiable."""
+        m = self.mu if mu is None else mu
+        total = None
+        for q, beam, of in zip(torch.split(m, self.sizes), self.plans, self.output_factors):
+            d = engine.photon_fluence_dose_autograd(q.reshape(beam.nb, beam.na), beam)
+            d = d * of if of != 1.0 else d
+            total = d if total is None else total + d
+        return total
+
+    def dose_list(self, mu=None):
+        raise NotImplementedError("fluence maps are optimised on the full volume")
 
 
 def save_influence_csr(path: str, row_ptr: torch.Tensor, col: torch.Tensor, val: torch.Tensor, shape, n_spots: int):

@@ -414,6 +414,15 @@ int dc_photon_beam_terma(dc_photon_beam *beam, const dc_photon_model *model, con
                          float *terma_out_dev, void *stream);
 /* Full CCCS dose of the last TERMA (as dc_photon_dose_dev). */
 int dc_photon_beam_dose(dc_photon_beam *beam, float *dose_out_dev, void *stream);
+/* No counterpart in the reference.  The CCCS of the beam's TERMA by
+ * cone-direction sweeps (an approximation of cccKernel, IMRTClasses.cu:
+ * 252-350): per cone direction, (TERMA, density) sampled once per node of a
+ * lattice of parallel lines one voxel apart over the irradiated region, the
+ * truncated recursions of every node from one warp-level scan along its line,
+ * and the result interpolated at each voxel.  Drops the per-voxel kernel tilt
+ * (:173-203) and interpolates between lines, so it is not held to the parity
+ * bar; isotropic grids only.  Synchronises `stream` once. */
+int dc_photon_beam_dose_sweep(dc_photon_beam *beam, float *dose_out_dev, void *stream);
 /* Probe voxels of a control point: rays from the source through the open
  * field's centre, half-field and edge positions, lateral profiles at three
  * depths, and every lattice_stride-th voxel along each axis (0: no lattice;

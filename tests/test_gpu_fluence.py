@@ -83,3 +83,28 @@ def test_central_differences_of_a_nonlinear_objective(setup):
             num = (objective(fp.reshape(F0.shape)) - objective(fm.reshape(F0.shape))).item() / (2 * h)
         scale = max(abs(num), 1e-3 * float(grad.abs().max()))
         assert abs(float(grad[q]) - num) <= 2e-3 * scale, (q, float(grad[q]), num)
+
+
+def test_fluence_optimizer_lowers_the_objective_and_resumes(setup, tmp_path):
+    torch, engine, grid, model, cp, density, fb = setup
+    from dosecuda_b200.optimize import DoseObjective, FluenceOptimizer
+    d0 = fb.dose(torch.ones((fb.nb, fb.na), device="cuda")).clone()
+    dmax = float(d0.max())
+    # flatten the dose inside the field's high-dose region to 90 % of Dmax
+    target = d0 > 0.5 * dmax
+    obj = DoseObjective().uniform(target, 0.9 * dmax)
+    opt = FluenceOptimizer([fb], obj, lr=0.05)
+    f0 = opt.evaluate()
+    opt.run(15)
+    f1 = opt.evaluate()
+    assert f1 < 0.7 * f0
+    ck = str(tmp_path / "fl.pt")
+    opt.save(ck)
+    opt.run(5)
+    after = opt.mu.detach().clone()
+    opt2 = FluenceOptimizer([fb], obj, lr=0.05)
+    opt2.load(ck)
+    opt2.run(5)
+    torch.cuda.synchronize()
+    # float atomics in the adjoint reorder between runs
+    assert float((opt2.mu.detach() - after).abs().max()) <= 1e-4 * float(after.abs().max())
