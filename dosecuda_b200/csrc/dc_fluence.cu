@@ -13,7 +13,7 @@
 // (the reference's TERMA mask, held fixed at the unmodulated TERMA).
 //
 //  * fluence_modulate_kernel writes m T0 into the CCCS's (TERMA, density)
-//    array (and its padded linear copy) and m E0 into the electron term; the
+//    array and m E0 into the electron term; the
 //    unchanged CCCS kernel then gives D.  F = 1 gives T0 and E0 bit for bit.
 //  * cccs_adjoint_kernel computes h = s K^T g: per voxel p with g(p) != 0
 //    and per direction, the recursion's sensitivity to each sample's TERMA,
@@ -41,7 +41,8 @@ constexpr int kMaxSmemBeamlets = 4096;  // float64 beamlet sums kept in shared m
 
 // Bilinear weights of the fluence map at the voxel's beam's-eye-view position
 // (clamped to the map's edge, so that a constant map gives that constant).
-__device__ __forceinline__ void fluence_taps(const FluenceMap &M, const Frame &f, float3 p, int idx[4], float w[4]) {
+__device__ __forceinline__ void fluence_taps(const FluenceMap &M, const Frame &f, float3 p, int idx[4], float w[4],
+                                             float *wa_out = nullptr, float *wb_out = nullptr) {
     const float3 h = image_to_head<true>(f, p);
     const float den = M.sad - h.z;
     float ua = (h.x * M.sad / den - M.a0) * M.inv_pitch;
@@ -59,6 +60,8 @@ __device__ __forceinline__ void fluence_taps(const FluenceMap &M, const Frame &f
     w[1] = wa * (1.0f - wb);
     w[2] = (1.0f - wa) * wb;
     w[3] = wa * wb;
+    if (wa_out) *wa_out = wa;
+    if (wb_out) *wb_out = wb;
 }
 
 }  // namespace
@@ -68,7 +71,7 @@ __global__ void __launch_bounds__(128) fluence_modulate_kernel(Grid g, Frame f, 
                                                                const float *__restrict__ T0,
                                                                const float *__restrict__ E0,
                                                                cudaTextureObject_t dens_tex,
-                                                               cudaSurfaceObject_t td_surf, float2 *__restrict__ td_lin,
+                                                               cudaSurfaceObject_t td_surf,
                                                                float *__restrict__ electron) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
@@ -77,25 +80,26 @@ __global__ void __launch_bounds__(128) fluence_modulate_kernel(Grid g, Frame f, 
     const long long v = (long long)i + (long long)g.nx * (j + (long long)g.ny * k);
     int idx[4];
     float w[4];
-    fluence_taps(M, f, voxel_xyz(g, f, i, j, k), idx, w);
+    float wa, wb;
+    fluence_taps(M, f, voxel_xyz(g, f, i, j, k), idx, w, &wa, &wb);
     const int nmap = M.na * M.nb;
-    float m = 0.0f;
+    float fv[4];
 #pragma unroll
-    for (int q = 0; q < 4; ++q) m = fmaf(w[q], DC_IN_BOUNDS(idx[q], nmap, 50) ? __ldg(F + idx[q]) : 0.0f, m);
+    for (int q = 0; q < 4; ++q) fv[q] = DC_IN_BOUNDS(idx[q], nmap, 50) ? __ldg(F + idx[q]) : 0.0f;
+    // bilinear as nested linear interpolations, so that a constant map gives
+    // exactly that constant (products of weights need not sum to 1 in float)
+    const float m0 = fmaf(wa, fv[1] - fv[0], fv[0]), m1 = fmaf(wa, fv[3] - fv[2], fv[2]);
+    const float m = fmaf(wb, m1 - m0, m0);
     const bool ok = DC_IN_BOUNDS(v, g.n(), 51);
     const float T = ok ? m * __ldg(T0 + v) : 0.0f;
     const float rho = tex3D<float>(dens_tex, (float)i + 0.5f, (float)j + 0.5f, (float)k + 0.5f);
     surf3Dwrite(make_float2(T, rho), td_surf, i * (int)sizeof(float2), j, k);
-    if (td_lin != nullptr) {
-        const long long pv = td_pad_index(g, i, j, k);
-        if (DC_IN_BOUNDS(pv, td_pad_count(g), 52)) td_lin[pv] = make_float2(T, rho);
-    }
     if (ok) electron[v] = m * __ldg(E0 + v);
 }
 
 __global__ void __launch_bounds__(128) cccs_adjoint_kernel(Grid g, Frame f, CccsCones C, float sp_cm, float scale,
                                                            const float4 *__restrict__ dirs,
-                                                           cudaTextureObject_t td_tex, const float2 *__restrict__ td_lin,
+                                                           cudaTextureObject_t td_tex,
                                                            const int *__restrict__ active,
                                                            const unsigned *__restrict__ n_active,
                                                            const float *__restrict__ grad_dose, float *__restrict__ h) {
@@ -144,8 +148,6 @@ __global__ void __launch_bounds__(128) cccs_adjoint_kernel(Grid g, Frame f, Cccs
                 r.x += ax.x * sc;
                 r.y += ax.y * sc;
                 r.z += ax.z * sc;
-                const int d = c * 12 + az;
-                const bool lsu = td_lin != nullptr && ((C.lsu_mask[d >> 5] >> (d & 31)) & 1u);
                 float Pe = 1.0f, Pb = 1.0f;  // products of the nearer samples' factors
                 for (int s = ns - 1; s >= 0; --s) {
                     const float rl10 = s_rl10[s0 + s];
@@ -154,7 +156,7 @@ __global__ void __launch_bounds__(128) cccs_adjoint_kernel(Grid g, Frame f, Cccs
                     q.y = fmaf(r.y, rl10, p.y);
                     q.z = fmaf(r.z, rl10, p.z);
                     const float3 tc = tex_coord(g, f, q);
-                    const float rho = lsu ? td_fetch_lin(td_lin, g, tc).y : tex3D<float2>(td_tex, tc.x, tc.y, tc.z).y;
+                    const float rho = tex3D<float2>(td_tex, tc.x, tc.y, tc.z).y;
                     const float Di = fmaxf(rho, kAirDensity) * sp_cm;
                     const float ex = fast_exp2(nam_l2e * Di);
                     const float wT = gp * (am * cp * (1.0f - ex) * Pe + bm * cs * Di * Pb);
@@ -248,10 +250,7 @@ static dim3 fl_grid(const Grid &g) {
 void enqueue_fluence_modulate(DeviceContext &ctx, const Grid &g, const Frame &f, const FluenceMap &M,
                               const float *F, const float *T0, const float *E0, const PhotonWork &w, cudaStream_t s) {
     KernelTimer kt(ctx, "fluence_modulate", s);
-    float2 *tl = (w.td_lin && w.td_lin->ptr && w.td_lin->bytes >= (size_t)td_pad_count(g) * sizeof(float2))
-                     ? w.td_lin->as<float2>()
-                     : nullptr;
-    fluence_modulate_kernel<<<fl_grid(g), dim3(32, 4, 1), 0, s>>>(g, f, M, F, T0, E0, w.dens_tex, w.td_surf, tl,
+    fluence_modulate_kernel<<<fl_grid(g), dim3(32, 4, 1), 0, s>>>(g, f, M, F, T0, E0, w.dens_tex, w.td_surf,
                                                                   w.electron);
     check_launch("fluence_modulate_kernel");
 }
@@ -259,9 +258,6 @@ void enqueue_fluence_modulate(DeviceContext &ctx, const Grid &g, const Frame &f,
 void enqueue_fluence_adjoint(DeviceContext &ctx, const Grid &g, const Frame &f, const CccsCones &C,
                              const FluenceMap &M, float dose_scale, const float *T0, const float *E0,
                              const PhotonWork &w, const float *grad_dose, float *h, double *grad_F, cudaStream_t s) {
-    const float2 *tl = (w.td_lin && w.td_lin->ptr && w.td_lin->bytes >= (size_t)td_pad_count(g) * sizeof(float2))
-                           ? w.td_lin->as<float2>()
-                           : nullptr;
     DC_CUDA(cudaMemsetAsync(h, 0, (size_t)g.n() * sizeof(float), s));
     DC_CUDA(cudaMemsetAsync(grad_F, 0, (size_t)M.na * M.nb * sizeof(double), s));
     {
@@ -271,7 +267,7 @@ void enqueue_fluence_adjoint(DeviceContext &ctx, const Grid &g, const Frame &f, 
         DC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cccs_adjoint_kernel, 128, 0));
         const long long want = (g.n() + 127) / 128;
         const unsigned blocks = (unsigned)std::max(1LL, std::min<long long>(want, (long long)sms * std::max(per_sm, 1)));
-        cccs_adjoint_kernel<<<blocks, 128, 0, s>>>(g, f, C, g.sx / 10.0f, dose_scale, w.dirs, w.td_tex, tl, w.active,
+        cccs_adjoint_kernel<<<blocks, 128, 0, s>>>(g, f, C, g.sx / 10.0f, dose_scale, w.dirs, w.td_tex, w.active,
                                                    w.n_active, grad_dose, h);
         check_launch("cccs_adjoint_kernel");
     }

@@ -37,7 +37,6 @@
 //  * The TERMA kernel maps threads to 32x4 voxel tiles (coalesced stores).
 #include <algorithm>
 #include <cmath>
-#include <cstdlib>
 #include <string>
 #include <vector>
 
@@ -134,22 +133,9 @@ __device__ __forceinline__ float head_transmission(const PhotonParams &P, float3
 // (warp-aggregated), so the CCCS runs on full warps of active voxels only.
 // dose (or null) receives the zero of masked voxels; terma_out (or null) a
 // linear copy of the TERMA volume.
-__global__ void td_shell_kernel(Grid g, float2 *__restrict__ td_lin) {
-    const long long total = td_pad_count(g);
-    const int px = g.nx + 3, py = g.ny + 3;
-    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < total;
-         q += (long long)gridDim.x * blockDim.x) {
-        const int ii = (int)(q % px);
-        const int jj = (int)((q / px) % py);
-        const int kk = (int)(q / ((long long)px * py));
-        if (ii == 0 || ii > g.nx || jj == 0 || jj > g.ny || kk == 0 || kk > g.nz)
-            td_lin[q] = make_float2(0.0f, kAirDensity);
-    }
-}
-
 __global__ void __launch_bounds__(128) terma_kernel(Grid g, Frame f, PhotonParams P, const float *__restrict__ wet,
                                                     cudaTextureObject_t dens_tex, cudaSurfaceObject_t td_surf,
-                                                    float2 *__restrict__ td_lin, float *__restrict__ electron,
+                                                    float *__restrict__ electron,
                                                     float *__restrict__ dose, float *__restrict__ terma_out,
                                                     int *__restrict__ active, unsigned *__restrict__ n_active) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -199,10 +185,6 @@ __global__ void __launch_bounds__(128) terma_kernel(Grid g, Frame f, PhotonParam
     const float T = oaf * ((1.0f - P.ssw) * tp * terma + P.ssw * ts * terma);
     const float rho = tex3D<float>(dens_tex, (float)i + 0.5f, (float)j + 0.5f, (float)k + 0.5f);
     surf3Dwrite(make_float2(T, rho), td_surf, i * (int)sizeof(float2), j, k);
-    if (td_lin != nullptr) {
-        const long long pv = td_pad_index(g, i, j, k);
-        if (DC_IN_BOUNDS(pv, td_pad_count(g), 14)) td_lin[pv] = make_float2(T, rho);
-    }
     const bool v_ok = DC_IN_BOUNDS(v, g.n(), 10);
     if (v_ok) electron[v] = P.esw * (0.4f + (0.3f * ratio)) * elec * tp;
     if (terma_out && v_ok) terma_out[v] = T;
@@ -250,11 +232,10 @@ __global__ void cone_dirs_kernel(Frame f, CccsCones C, float4 *__restrict__ dirs
 // kernel (every lane of a warp does a full 72-direction march).
 __device__ __forceinline__ float cccs_voxel(const Grid &g, const Frame &f, const CccsCones &C, float sp_cm,
                                             const float4 *s_dir, const float *s_rl10, cudaTextureObject_t td_tex,
-                                            const float2 *td_lin, float3 p);
+                                            float3 p);
 
 __global__ void __launch_bounds__(128) cccs_kernel(Grid g, Frame f, CccsCones C, float sp_cm, float dose_scale,
                                                    const float4 *__restrict__ dirs, cudaTextureObject_t td_tex,
-                                                   const float2 *__restrict__ td_lin,
                                                    const float *__restrict__ electron, const int *__restrict__ active,
                                                    const unsigned *__restrict__ n_active, float *__restrict__ dose) {
     __shared__ float4 s_dir[kMaxCones * 12];
@@ -274,7 +255,7 @@ __global__ void __launch_bounds__(128) cccs_kernel(Grid g, Frame f, CccsCones C,
         const int j = rem / g.nx;
         const int i = rem - j * g.nx;
         const float3 p = voxel_xyz(g, f, i, j, k);
-        float dose_value = cccs_voxel(g, f, C, sp_cm, s_dir, s_rl10, td_tex, td_lin, p);
+        float dose_value = cccs_voxel(g, f, C, sp_cm, s_dir, s_rl10, td_tex, p);
         dose_value += __ldg(electron + v);
         dose[v] = (!isnan(dose_value) && dose_value >= 0.0f) ? dose_scale * dose_value : 0.0f;  // v checked above
     }
@@ -284,7 +265,6 @@ __global__ void __launch_bounds__(128) cccs_kernel(Grid g, Frame f, CccsCones C,
 // per-voxel sum as cccs_kernel, with the mask taken from the TERMA texel.
 __global__ void __launch_bounds__(128) cccs_points_kernel(Grid g, Frame f, CccsCones C, float sp_cm, float dose_scale,
                                                           const float4 *__restrict__ dirs, cudaTextureObject_t td_tex,
-                                                          const float2 *__restrict__ td_lin,
                                                           const float *__restrict__ electron,
                                                           const int *__restrict__ voxels, int n,
                                                           float *__restrict__ out) {
@@ -309,7 +289,7 @@ __global__ void __launch_bounds__(128) cccs_points_kernel(Grid g, Frame f, CccsC
         float r = 0.0f;
         if (!(T <= 0.01f)) {
             const float3 p = voxel_xyz(g, f, i, j, k);
-            float dose_value = cccs_voxel(g, f, C, sp_cm, s_dir, s_rl10, td_tex, td_lin, p);
+            float dose_value = cccs_voxel(g, f, C, sp_cm, s_dir, s_rl10, td_tex, p);
             dose_value += __ldg(electron + v);
             r = (!isnan(dose_value) && dose_value >= 0.0f) ? dose_scale * dose_value : 0.0f;
         }
@@ -321,7 +301,7 @@ __global__ void __launch_bounds__(128) cccs_points_kernel(Grid g, Frame f, CccsC
 // (IMRTClasses.cu:289-339) for the voxel at image position p.
 __device__ __forceinline__ float cccs_voxel(const Grid &g, const Frame &f, const CccsCones &C, float sp_cm,
                                             const float4 *s_dir, const float *s_rl10, cudaTextureObject_t td_tex,
-                                            const float2 *td_lin, float3 p) {
+                                            float3 p) {
     // kernelTilt (IMRTClasses.cu:173-203): rotate each direction by the
     // rotation taking the central axis (iso -> source) onto voxel -> source.
     const float3 uvec = unit_to_source(f, p);
@@ -354,9 +334,6 @@ __device__ __forceinline__ float cccs_voxel(const Grid &g, const Frame &f, const
             r.y += ax.y * sc;
             r.z += ax.z * sc;
 
-            // warp-uniform: every lane takes the same direction
-            const int d = c * 12 + az;
-            const bool lsu = td_lin != nullptr && ((C.lsu_mask[d >> 5] >> (d & 31)) & 1u);
             float Rp = 0.0f, Rs = 0.0f;
             for (int s = 0; s < ns; ++s) {
                 const float rl10 = s_rl10[s0 + s];
@@ -365,7 +342,7 @@ __device__ __forceinline__ float cccs_voxel(const Grid &g, const Frame &f, const
                 q.y = fmaf(r.y, rl10, p.y);
                 q.z = fmaf(r.z, rl10, p.z);
                 const float3 tc = tex_coord(g, f, q);
-                const float2 td = lsu ? td_fetch_lin(td_lin, g, tc) : tex3D<float2>(td_tex, tc.x, tc.y, tc.z);
+                const float2 td = tex3D<float2>(td_tex, tc.x, tc.y, tc.z);
                 const float Ti = td.x;
                 const float Di = fmaxf(td.y, kAirDensity) * sp_cm;
                 const float ex = fast_exp2(nam_l2e * Di);
@@ -465,19 +442,6 @@ void build_photon_params(const dc_photon_model &m, const dc_control_point &cp, f
         off += n;
     }
     C.total_steps = off;
-    // Directions sampled in software (load/store path) rather than by the
-    // texture unit: none by default.  DC_CCCS_LSU_AZIMUTHS (12-bit mask, hex)
-    // and DC_CCCS_LSU_CONES (mask over the zenith cones, hex) select them.
-    unsigned az_mask = 0x000u, cone_mask = 0xFFu;
-    if (const char *e = std::getenv("DC_CCCS_LSU_AZIMUTHS")) az_mask = (unsigned)std::strtoul(e, nullptr, 16) & 0xFFFu;
-    if (const char *e = std::getenv("DC_CCCS_LSU_CONES")) cone_mask = (unsigned)std::strtoul(e, nullptr, 16) & 0xFFu;
-    C.lsu_mask[0] = C.lsu_mask[1] = C.lsu_mask[2] = 0u;
-    for (int c = 0; c < C.n_cones; ++c)
-        for (int az = 0; az < 12; ++az)
-            if (((cone_mask >> c) & 1u) && ((az_mask >> az) & 1u)) {
-                const int d = c * 12 + az;
-                C.lsu_mask[d >> 5] |= 1u << (d & 31);
-            }
 }
 
 static unsigned cccs_blocks(const DeviceContext &ctx, long long work) {
@@ -491,24 +455,8 @@ static unsigned cccs_blocks(const DeviceContext &ctx, long long work) {
 
 DC_BOUNDS_TAKE(take_bounds_photon)
 
-// The padded linear (TERMA, density) copy of this work set, when it has one
-// of the grid's size (ensured by enqueue_terma).
-static float2 *td_lin_ptr(const Grid &g, const PhotonWork &w) {
-    if (w.td_lin == nullptr || w.td_lin->ptr == nullptr ||
-        w.td_lin->bytes < (size_t)td_pad_count(g) * sizeof(float2))
-        return nullptr;
-    return w.td_lin->as<float2>();
-}
-
 void enqueue_terma(DeviceContext &ctx, const Grid &g, const Frame &f, const PhotonParams &P, const CccsCones &C,
                    const PhotonWork &w, float *dose_dev, float *terma_out, cudaStream_t s) {
-    if (w.td_lin != nullptr) {
-        // border shell of the padded copy (the TERMA kernel writes the interior)
-        float2 *tl = static_cast<float2 *>(w.td_lin->ensure((size_t)td_pad_count(g) * sizeof(float2)));
-        const long long cells = td_pad_count(g);
-        td_shell_kernel<<<(unsigned)std::min<long long>((cells + 255) / 256, 4096), 256, 0, s>>>(g, tl);
-        check_launch("td_shell_kernel");
-    }
     if (g.n() > 0x7fffffffLL) throw Error(DC_ERR_VALUE, "photon volumes are limited to 2^31 - 1 voxels.");
     if (w.depth_mode == 1 && w.xlat != nullptr)
         launch_xray_depth(ctx, g, f, w.dens_tex, w.wet, w.active, w.n_active, *w.xlat, w.depth_stats,
@@ -520,8 +468,7 @@ void enqueue_terma(DeviceContext &ctx, const Grid &g, const Frame &f, const Phot
     DC_CUDA(cudaMemsetAsync(w.n_active, 0, sizeof(unsigned), s));
     {
         KernelTimer kt(ctx, "terma", s);
-        terma_kernel<<<vol_grid(g), dim3(32, 4, 1), 0, s>>>(g, f, P, w.wet, w.dens_tex, w.td_surf,
-                                                            td_lin_ptr(g, w), w.electron,
+        terma_kernel<<<vol_grid(g), dim3(32, 4, 1), 0, s>>>(g, f, P, w.wet, w.dens_tex, w.td_surf, w.electron,
                                                             dose_dev, terma_out, w.active, w.n_active);
         check_launch("terma_kernel");
     }
@@ -533,7 +480,6 @@ void enqueue_cccs(DeviceContext &ctx, const Grid &g, const Frame &f, const CccsC
                   float dose_scale, float *dose_dev, cudaStream_t s) {
     KernelTimer kt(ctx, "cccs", s);
     cccs_kernel<<<cccs_blocks(ctx, g.n()), 128, 0, s>>>(g, f, C, g.sx / 10.0f, dose_scale, w.dirs, w.td_tex,
-                                                        td_lin_ptr(g, w),
                                                         w.electron, w.active, w.n_active, dose_dev);
     check_launch("cccs_kernel");
 }
@@ -543,8 +489,7 @@ void enqueue_cccs_points(DeviceContext &ctx, const Grid &g, const Frame &f, cons
     if (n <= 0) return;
     KernelTimer kt(ctx, "cccs_points", s);
     cccs_points_kernel<<<cccs_blocks(ctx, n), 128, 0, s>>>(g, f, C, g.sx / 10.0f, dose_scale, w.dirs, w.td_tex,
-                                                           td_lin_ptr(g, w),
-                                                           w.electron, voxels, n, out);
+                                                              w.electron, voxels, n, out);
     check_launch("cccs_points_kernel");
 }
 
@@ -568,7 +513,6 @@ void run_photon_pipeline(DeviceContext &ctx, const Grid &g, const Frame &f, cons
     w.n_active = reinterpret_cast<unsigned *>(act);
     w.active = reinterpret_cast<int *>(act + 256);
     w.xlat = &ctx.xlat;
-    w.td_lin = &ctx.td_lin;
     w.depth_mode = ctx.photon_depth_mode;
     w.depth_stats = static_cast<unsigned *>(ctx.xstat.ensure(sizeof(unsigned)));
     enqueue_terma(ctx, g, f, P, C, w, dose_dev, nullptr, s);

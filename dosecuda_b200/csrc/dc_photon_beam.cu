@@ -36,7 +36,7 @@ struct dc_photon_beam {
     float origin[3] = {0, 0, 0};
     VolumeArray density;
     VolumeArray td;
-    DeviceBuffer wet, electron, active, dirs, probe, xlat, td_lin;
+    DeviceBuffer wet, electron, active, dirs, probe, xlat;
     // fluence mode: the unmodulated TERMA and electron term of the last
     // dc_photon_beam_terma, and the adjoint's scratch
     DeviceBuffer terma0, electron0, fl_h;
@@ -67,7 +67,6 @@ struct dc_photon_beam {
         w.td_surf = td.surf;
         w.td_tex = td.texture(0.0f, kAirDensity);
         w.xlat = &xlat;
-        w.td_lin = &td_lin;
         w.depth_mode = context(device).photon_depth_mode;
         return w;
     }
@@ -77,7 +76,6 @@ struct dc_photon_beam {
         td.release();
         wet.release();
         xlat.release();
-        td_lin.release();
         terma0.release();
         electron0.release();
         fl_h.release();

@@ -318,6 +318,7 @@ __device__ __forceinline__ void pb_tile(const Grid &g, const Frame &f, const Pro
     __shared__ float s_red[TY][6];
     __shared__ float s_bb[6];
     __shared__ int s_wcnt[TY];
+    __shared__ float s_sig[TY];
     {
         float b[6] = {INFINITY, -INFINITY, INFINITY, -INFINITY, INFINITY, -INFINITY};
 #pragma unroll
@@ -404,7 +405,27 @@ __device__ __forceinline__ void pb_tile(const Grid &g, const Frame &f, const Pro
         const bool block_any = __syncthreads_or(any);
         if (!block_any) continue;
 
-        const float rcut2 = L.rcut * L.rcut;
+        // Lateral cut-off of this CTA for this layer: 6 x the widest halo
+        // sigma of its active voxels (sigma_ht^2 = -log2(e) / (2 hs2)), never
+        // wider than the layer's bound.  A spot whose axis stays farther than
+        // that from the CTA's box lies beyond 6 sigma_ht of every voxel here,
+        // where both Gaussians are below exp(-18) of their peaks.
+        float rcut2;
+        {
+            float s2 = 0.0f;
+#pragma unroll
+            for (int v = 0; v < VY; ++v)
+                if (act[v] && pv[v].hs2 < 0.0f) s2 = fmaxf(s2, -0.5f * kLog2e / pv[v].hs2);
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) s2 = fmaxf(s2, __shfl_xor_sync(0xffffffffu, s2, o));
+            if (lane == 0) s_sig[threadIdx.y] = s2;
+            __syncthreads();
+            float m2 = s_sig[0];
+#pragma unroll
+            for (int w = 1; w < TY; ++w) m2 = fmaxf(m2, s_sig[w]);
+            const float rc = 6.0f * (sqrtf(m2) * 1.01f + 0.1f);
+            rcut2 = fminf(L.rcut * L.rcut, rc * rc);
+        }
         for (int c0 = 0; c0 < L.n_spots; c0 += kPbSpotChunk) {
             const int craw = min(kPbSpotChunk, L.n_spots - c0);
             if (c0 > 0) __syncthreads();

@@ -224,7 +224,6 @@ void DeviceContext::release_all() {
     active.release();
     xlat.release();
     xstat.release();
-    td_lin.release();
     small.release();
     lut.release();
     tables.release();

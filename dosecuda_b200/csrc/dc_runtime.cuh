@@ -121,13 +121,12 @@ class DeviceContext {
     DeviceBuffer tables;      // proton layer + spot tables
     DeviceBuffer xlat;        // photon ray-lattice integrals G[node][ray] (dc_xray.cu)
     DeviceBuffer xstat;       // voxels the last photon depth pass marched exactly
-    DeviceBuffer td_lin;      // padded linear (TERMA, density) copy for the CCCS's software samples
     VolumeArray density;      // density / RLSP texture
     VolumeArray terma;        // TERMA texture (surface-writable)
     // Photon radiological depth: 0 = the reference's per-voxel 1 mm march,
     // 1 = the beam's-eye-view ray lattice (dc_xray.cu).  Set by
     // dc_photon_set_depth_mode; read when a photon call is enqueued.
-    int photon_depth_mode = 0;
+    int photon_depth_mode = 1;
     // Ring of pinned staging slots for per-call tables: the host reuses a slot
     // only after the copy out of it (event) has completed.
     static constexpr int kPinSlots = 4;

@@ -114,7 +114,7 @@ PHOTON_DEPTH_MODES = {"march": 0, "lattice": 1}
 
 def photon_depth_mode(gpu_id: int = 0, mode: str | None = None) -> str:
     """Select how photon calls on ``gpu_id`` compute the radiological depth
-    ("march": the reference's per-voxel 1 mm march, the default; "lattice":
+    ("march": the reference's per-voxel 1 mm march; "lattice": the default,
     the beam's-eye-view ray lattice with the march as its fallback) and
     return the mode in force."""
     lib = _lib.load()

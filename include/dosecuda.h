@@ -150,9 +150,9 @@ int dc_release_device(int gpu_id);
 /* No counterpart in the reference (its ray trace, CudaClasses.cu:180-228,
  * is the only mode).  How photon calls on gpu_id compute the radiological
  * depth that TERMA attenuates with:
- *   DC_DEPTH_MARCH   (0): the default: the reference's per-voxel 1 mm
- *                         march, sample for sample;
- *   DC_DEPTH_LATTICE (1): the density integrated once along a
+ *   DC_DEPTH_MARCH   (0): the reference's per-voxel 1 mm march, sample
+ *                         for sample;
+ *   DC_DEPTH_LATTICE (1): the default: the density integrated once along a
  *                         beam's-eye-view lattice of rays from the source and
  *                         interpolated per voxel, with the reference's exact
  *                         sample count, its boundary samples fetched exactly,

@@ -2,7 +2,8 @@
 gamma index used as parity criteria.
 
 * ``dose_diff``: max |a - b| over voxels with b above ``thresh`` x max(b),
-  as a fraction of max(b) (the criterion |dD| <= 0.5 % Dmax above 10 % Dmax).
+  as a fraction of max(b) (the criterion |dD| <= 0.5 % Dmax above 10 % Dmax);
+  optionally over a voxel subset.
 * ``gamma_pass_rate``: global gamma (dose difference ``dd`` of max(ref),
   distance to agreement ``dta_mm``), evaluated at voxels where ref is above
   ``thresh`` x max(ref); the search is over whole-voxel shifts within
@@ -27,20 +28,26 @@ def wet_close(a, b):
     return bool(d.max() <= WET_MAX_CM and np.mean(d <= WET_CLOSE_CM) >= WET_CLOSE_FRAC)
 
 
-def dose_diff(a, b, thresh=0.10):
+def dose_diff(a, b, thresh=0.10, where=None, dmax=None):
+    """With ``where`` (boolean volume) only those voxels count, and ``dmax``
+    (default: max of b over them) normalises."""
     a = np.asarray(a, np.float64)
     b = np.asarray(b, np.float64)
-    m = float(np.abs(b).max())
+    sel = np.ones(b.shape, bool) if where is None else np.asarray(where, bool)
+    m = float(np.abs(b[sel]).max()) if dmax is None else float(dmax)
     if m == 0.0:
-        return float(np.abs(a).max())
-    mask = b > thresh * m
+        return float(np.abs(a[sel]).max())
+    mask = (b > thresh * m) & sel
     return float(np.abs(a - b)[mask].max() / m) if mask.any() else 0.0
 
 
-def gamma_pass_rate(test, ref, spacing_mm, dd=0.02, dta_mm=2.0, thresh=0.10):
+def gamma_pass_rate(test, ref, spacing_mm, dd=0.02, dta_mm=2.0, thresh=0.10, where=None, dmax=None):
+    """With ``where`` only those reference voxels are evaluated, and ``dmax``
+    (default: max of ref over them) is the dose criterion's normalisation."""
     test = np.asarray(test, np.float64)
     ref = np.asarray(ref, np.float64)
-    dmax = float(ref.max())
+    sel = np.ones(ref.shape, bool) if where is None else np.asarray(where, bool)
+    dmax = float(ref[sel].max()) if dmax is None else float(dmax)
     sp = np.broadcast_to(np.asarray(spacing_mm, np.float64), (3,))[::-1]  # (z, y, x)
     reach = [int(np.ceil(1.5 * dta_mm / s)) for s in sp]
     best = np.full(ref.shape, np.inf)
@@ -57,5 +64,5 @@ def gamma_pass_rate(test, ref, spacing_mm, dd=0.02, dta_mm=2.0, thresh=0.10):
                         reach[2] + dx:reach[2] + dx + nx]
                 g2 = ((sh - ref) / (dd * dmax)) ** 2 + r2 / dta_mm ** 2
                 np.minimum(best, g2, out=best)
-    mask = ref > thresh * dmax
+    mask = (ref > thresh * dmax) & sel
     return float((best[mask] <= 1.0).mean()) if mask.any() else 1.0

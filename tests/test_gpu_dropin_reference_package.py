@@ -1,6 +1,8 @@
 """The drop-in claim on the reference's own package: its unmodified plan
 modules (installed from the reference sources into baseline/_ref) compute the
-config-1 proton plan and a two-beam photon plan through their public API,
+config-1 proton plan and a two-beam photon plan (40 x 40 cm fields over the
+128^3 photon phantom, where the reference's TERMA is sound everywhere) through
+their public API,
 once with their own compiled ``dose_kernels`` and once with
 ``sys.modules["dose_kernels"] = dosecuda_b200.dose_kernels`` set before the
 package is imported.  The doses must agree within the parity bar.  Each run is
@@ -43,8 +45,7 @@ def test_reference_package_binds_engine_and_matches(tmp_path):
     inp = str(tmp_path / "inputs.npz")
     np.savez(inp, p_hu=pg.HU, p_origin=np.asarray(pg.origin, np.float64), p_spacing=np.asarray(pg.spacing, np.float64),
              p_spots=pb.spot_list, p_angles=np.array([pb.gantry_angle, pb.couch_angle]), p_iso=pb.iso,
-             x_hu=xg.HU, x_origin=np.asarray(xg.origin, np.float64), x_spacing=np.asarray(xg.spacing, np.float64),
-             x_iso_shift=np.float32([0.5 * xg.spacing[0], 0.0, 0.0]))
+             x_hu=xg.HU, x_origin=np.asarray(xg.origin, np.float64), x_spacing=np.asarray(xg.spacing, np.float64))
     eng = _run("engine", inp, str(tmp_path / "engine.npz"))
     ref = _run("reference", inp, str(tmp_path / "reference.npz"))
     # which extension each run bound

@@ -107,9 +107,9 @@ def test_lattice_dose_matches_march_and_oracle(engine, name):
 
 
 def test_lattice_dose_vs_reference_build_whole_volume(engine):
-    """The 128^3 workload with the isocentre half a voxel off the grid (where
-    the reference's TERMA is sound, test_gpu_reference_terma.py): the engine
-    in lattice mode against the reference's build on every voxel."""
+    """The 128^3 workload with every leaf pair open over the phantom (where
+    the reference's TERMA is sound on every voxel, test_gpu_reference_terma.py):
+    the engine in lattice mode against the reference's build on every voxel."""
     ref_dir = os.path.join(ROOT, "oracle", "_ref")
     if not glob.glob(os.path.join(ref_dir, "dose_kernels*.so")):
         pytest.skip("reference build oracle/_ref not present")
@@ -117,9 +117,9 @@ def test_lattice_dose_vs_reference_build_whole_volume(engine):
     import dose_kernels as ref
     sys.path.remove(ref_dir)
     from dosecuda_b200 import phantoms
-    grid, plan, model, cp, density = _case("small_photon_128")
-    cp.iso = np.array(cp.iso, np.float32) + np.float32([0.5 * grid.spacing[0], 0.0, 0.0])
-    vol = phantoms.volume_object(grid, density)
+    grid, plan = phantoms.photon_small(field_cm=(40.0, 40.0))
+    model, cp = plan.beam_models[0], plan.beam_list[0].cp_list[0]
+    vol = phantoms.volume_object(grid, grid.DensityFromHU(plan.machine_name))
     engine.photon_depth_mode(0, "lattice")
     from dosecuda_b200 import dose_kernels as dk
     d = dk.photon_dose_cuda(model, vol, cp, 0)
