@@ -41,7 +41,7 @@ PEAKS_FALLBACK = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
 # until it is captured again.
 NCU_TRAFFIC = {
     "cccs": (15102976, "profiles/cccs_photon_small.md"),
-    "pencil_beam": (3622400, "profiles/pencil_beam_proton_small.md"),
+    "pencil_beam": (3622912, "profiles/pencil_beam_proton_small.md"),
     "conv_dec0": (67162880 + 26884352, "profiles/conv_gather_dec0_surrogate_128.md"),
 }
 SM_COUNT = 148
@@ -1089,7 +1089,7 @@ def main():
     ap.add_argument("--batch-plans", type=int, default=16, help="plans in the batched workload (0: skip)")
     ap.add_argument("--opt-iters", type=int, default=200, help="optimisation iterations (0: skip)")
     ap.add_argument("--tune-cache", action="store_true", help="keep the tile autotuner's JSON cache")
-    ap.add_argument("--surrogate-beams", type=int, default=30, help="held-out beams for the surrogate (0: skip)")
+    ap.add_argument("--surrogate-beams", type=int, default=300, help="held-out beams for the surrogate (0: skip)")
     ap.add_argument("--no-plan-loop", dest="plan_loop", action="store_false",
                     help="skip the 18-control-point IMRT plan")
     args = ap.parse_args()

@@ -238,7 +238,7 @@ int dc_proton_raytrace(int gpu_id, const float *rlsp, int nz, int ny, int nx, co
         const Grid g = make_grid(nz, ny, nx, spacing);
         const Frame f = make_frame(iso, origin, gantry_deg, couch_deg, 0.0, (vsadx + vsady) / 2.0f);
         ctx.density.ensure(nx, ny, nz, false);
-        copy_host_to_array(ctx.density, rlsp, nz, ny, nx, cudaMemcpyHostToDevice, s);
+        upload_host_volume(ctx, rlsp, nz, ny, nx, &ctx.density, nullptr, s);
         const size_t vb = (size_t)g.n() * sizeof(float);
         // page-locked output: the smoothing kernel stores into it directly
         float *direct = static_cast<float *>(mapped_host_range(wet_out, vb));
@@ -301,7 +301,7 @@ int dc_proton_spot(int gpu_id, const float *wet, int nz, int ny, int nx, const f
         const size_t lb = (size_t)n_energies * lut_len * sizeof(float);
         const size_t lb_al = (lb + 255) & ~(size_t)255;
         char *lut = static_cast<char *>(ctx.lut.ensure(3 * lb_al));
-        if (!wet_direct) DC_CUDA(cudaMemcpyAsync(wet_d, wet, vb, cudaMemcpyHostToDevice, s));
+        if (!wet_direct) upload_host_volume(ctx, wet, nz, ny, nx, nullptr, wet_d, s);
         DC_CUDA(cudaMemcpyAsync(lut, lut_depths, lb, cudaMemcpyHostToDevice, s));
         DC_CUDA(cudaMemcpyAsync(lut + lb_al, lut_sigmas, lb, cudaMemcpyHostToDevice, s));
         DC_CUDA(cudaMemcpyAsync(lut + 2 * lb_al, lut_idds, lb, cudaMemcpyHostToDevice, s));
@@ -397,7 +397,7 @@ int dc_photon_dose(int gpu_id, const float *density, int nz, int ny, int nx, con
         const Frame f = make_frame(cp->iso, origin, cp->gantry_deg, cp->couch_deg, cp->collimator_deg,
                                    model->primary_source_distance);
         ctx.density.ensure(nx, ny, nz, false);
-        copy_host_to_array(ctx.density, density, nz, ny, nx, cudaMemcpyHostToDevice, s);
+        upload_host_volume(ctx, density, nz, ny, nx, &ctx.density, nullptr, s);
         const size_t vb = (size_t)g.n() * sizeof(float);
         // page-locked output: TERMA (masked zeros) and CCCS store into it directly
         float *direct = static_cast<float *>(mapped_host_range(dose_out, vb));

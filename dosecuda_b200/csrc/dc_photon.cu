@@ -234,7 +234,7 @@ __device__ __forceinline__ float cccs_voxel(const Grid &g, const Frame &f, const
                                             const float4 *s_dir, const float *s_rl10, cudaTextureObject_t td_tex,
                                             float3 p);
 
-__global__ void __launch_bounds__(128) cccs_kernel(Grid g, Frame f, CccsCones C, float sp_cm, float dose_scale,
+__global__ void __launch_bounds__(128, 10) cccs_kernel(Grid g, Frame f, CccsCones C, float sp_cm, float dose_scale,
                                                    const float4 *__restrict__ dirs, cudaTextureObject_t td_tex,
                                                    const float *__restrict__ electron, const int *__restrict__ active,
                                                    const unsigned *__restrict__ n_active, float *__restrict__ dose) {
@@ -310,6 +310,12 @@ __device__ __forceinline__ float cccs_voxel(const Grid &g, const Frame &f, const
     const float3 ax = make_float3(axis0.y * uvec.z - axis0.z * uvec.y, axis0.z * uvec.x - axis0.x * uvec.z,
                                   axis0.x * uvec.y - axis0.y * uvec.x);
     const float inv1c = 1.0f / (1.0f + costh);
+    // A sample at distance 0 lies on the voxel centre whatever the direction
+    // (fmaf(r, 0, p) == p), so every cone whose sample distances end exactly
+    // at 0 fetches the same texel there: fetched once here and reused,
+    // which gives the same value as the 72 separate fetches.
+    const float3 tc0 = tex_coord(g, f, p);
+    const float2 td0 = tex3D<float2>(td_tex, tc0.x, tc0.y, tc0.z);
 
     float dose_value = 0.0f;
     for (int c = 0; c < C.n_cones; ++c) {
@@ -342,7 +348,7 @@ __device__ __forceinline__ float cccs_voxel(const Grid &g, const Frame &f, const
                 q.y = fmaf(r.y, rl10, p.y);
                 q.z = fmaf(r.z, rl10, p.z);
                 const float3 tc = tex_coord(g, f, q);
-                const float2 td = tex3D<float2>(td_tex, tc.x, tc.y, tc.z);
+                const float2 td = rl10 == 0.0f ? td0 : tex3D<float2>(td_tex, tc.x, tc.y, tc.z);
                 const float Ti = td.x;
                 const float Di = fmaxf(td.y, kAirDensity) * sp_cm;
                 const float ex = fast_exp2(nam_l2e * Di);

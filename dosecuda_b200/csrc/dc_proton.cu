@@ -179,9 +179,13 @@ __device__ __forceinline__ float2 exp2_pair(float2 x) { return make_float2(fast_
 //  * |sigma_air| by the quadratic's extremes over the range of
 //    d = |voxel - source| - w + 0.7 R80 for voxels of the volume;
 //  * sigma_h by sampling the halo formula over [0.1, R80 - 0.1] mm.
-__global__ void layer_rcut_kernel(Grid g, Frame f, LayerRec *layers, int n_layers, const float *lut_depths,
-                                  const float *lut_sigmas, int lut_len) {
-    const int l = blockIdx.x * blockDim.x + threadIdx.x;
+// One warp per layer: the lanes share the LUT scan and the halo-sigma
+// samples, and the maxima are combined with shuffles.
+__global__ void __launch_bounds__(32) layer_rcut_kernel(Grid g, Frame f, LayerRec *layers, int n_layers,
+                                                        const float *lut_depths, const float *lut_sigmas,
+                                                        int lut_len) {
+    const int l = blockIdx.x;
+    const int lane = threadIdx.x;
     if (l >= n_layers) return;
     LayerRec &L = layers[l];
     // source distance range over the volume's bounding box (image frame, relative to iso)
@@ -198,11 +202,36 @@ __global__ void layer_rcut_kernel(Grid g, Frame f, LayerRec *layers, int n_layer
     const float wmax = 1.1f * r80;
     const float *D = lut_depths + (size_t)L.energy_id * lut_len;
     const float *S = lut_sigmas + (size_t)L.energy_id * lut_len;
-    float smcs = 0.f;
-    for (int q = 0; q < lut_len; ++q) {
-        smcs = fmaxf(smcs, fabsf(S[q]));
-        if (D[q] > wmax) break;  // the row bracketing wmax from above is included
+    // |sigma| over the rows up to the first one deeper than wmax (that row
+    // included: it brackets wmax from above)
+    int q_end = lut_len;
+    for (int q0 = 0; q0 < lut_len; q0 += 32) {
+        const int q = q0 + lane;
+        const bool deeper = q < lut_len && D[q] > wmax;
+        const unsigned m = __ballot_sync(0xffffffffu, deeper);
+        if (m) {
+            q_end = q0 + __ffs(m);  // one past the first deeper row
+            break;
+        }
     }
+    float smcs = 0.f;
+    for (int q = lane; q < q_end; q += 32) smcs = fmaxf(smcs, fabsf(S[q]));
+    // the halo sigma sampled over [0.1, R80 - 0.1] mm in 0.25 mm steps
+    float sh = 0.f;
+    const int n_w = r80 - 0.1f >= 0.1f ? (int)floorf((r80 - 0.2f) / 0.25f) + 1 : 0;
+    for (int q = lane; q < n_w; q += 32) {
+        const float w = 0.1f + 0.25f * (float)q;
+        if (w > r80 - 0.1f) break;
+        const float h = 2.85f + (0.0014f * r80 * logf(w + 3.0f)) + (0.06f * w) - (7.4e-5f * sqr(w)) -
+                        ((0.22f * r80) / sqr(w - r80 - 5.0f));
+        sh = fmaxf(sh, h);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        smcs = fmaxf(smcs, __shfl_xor_sync(0xffffffffu, smcs, o));
+        sh = fmaxf(sh, __shfl_xor_sync(0xffffffffu, sh, o));
+    }
+    if (lane != 0) return;
     const float d0 = sqrtf(dmin2) - wmax + 0.7f * r80 - 1.0f;
     const float d1 = sqrtf(dmax2) + 0.5f + 0.7f * r80 + 1.0f;
     auto sair = [&](float d) { return fabsf(fmaf(fmaf(L.A, d, L.B), d, L.C)); };
@@ -211,12 +240,6 @@ __global__ void layer_rcut_kernel(Grid g, Frame f, LayerRec *layers, int n_layer
         const float dv = -L.B / (2.0f * L.A);
         if (dv > d0 && dv < d1) sa = fmaxf(sa, sair(dv));
     }
-    float sh = 0.f;
-    for (float w = 0.1f; w <= r80 - 0.1f; w += 0.25f) {
-        const float h = 2.85f + (0.0014f * r80 * logf(w + 3.0f)) + (0.06f * w) - (7.4e-5f * sqr(w)) -
-                        ((0.22f * r80) / sqr(w - r80 - 5.0f));
-        sh = fmaxf(sh, h);
-    }
     const float sht = hypotf(sa + smcs, sh * 1.02f + 0.2f) * 1.01f + 0.5f;
     L.rcut = (sht == sht) ? 6.0f * sht : INFINITY;
 }
@@ -224,7 +247,7 @@ __global__ void layer_rcut_kernel(Grid g, Frame f, LayerRec *layers, int n_layer
 void launch_layer_rcut(const Grid &g, const Frame &f, LayerRec *layers, int n_layers, const float *lut_depths,
                        const float *lut_sigmas, int lut_len, cudaStream_t s) {
     if (n_layers <= 0) return;
-    layer_rcut_kernel<<<(n_layers + 63) / 64, 64, 0, s>>>(g, f, layers, n_layers, lut_depths, lut_sigmas, lut_len);
+    layer_rcut_kernel<<<n_layers, 32, 0, s>>>(g, f, layers, n_layers, lut_depths, lut_sigmas, lut_len);
     check_launch("layer_rcut_kernel");
 }
 

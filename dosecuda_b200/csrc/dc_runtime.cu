@@ -1,5 +1,8 @@
 // dc_runtime.cu — device contexts, cached buffers and textures, profiler.
 #include <atomic>
+#include <algorithm>
+#include <condition_variable>
+#include <thread>
 #include <cstdlib>
 #include <cuda.h>
 
@@ -194,6 +197,7 @@ DeviceContext::DeviceContext(int dev) : device(dev) {
     DC_CUDA(cudaSetDevice(dev));
     DC_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
     for (auto &e : pin_ev) DC_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    for (auto &e : stage_ev) DC_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     DC_CUDA(cudaEventCreateWithFlags(&last_use, cudaEventDisableTiming));
 }
 
@@ -238,6 +242,11 @@ void DeviceContext::release_all() {
     for (auto e : event_pool) cudaEventDestroy(e);
     event_pool.clear();
     for (auto &e : pin_ev) {
+        if (e) cudaEventDestroy(e);
+        e = nullptr;
+    }
+    for (auto &b : stage) b.release();
+    for (auto &e : stage_ev) {
         if (e) cudaEventDestroy(e);
         e = nullptr;
     }
@@ -355,6 +364,121 @@ Grid make_grid(int nz, int ny, int nx, const float spacing[3]) {
     g.inv_sy = 1.0f / g.sy;
     g.inv_sz = 1.0f / g.sz;
     return g;
+}
+
+// ---------------------------------------------------------------------------
+// Parallel host copies for pageable uploads: a few persistent worker threads
+// (kept for the life of the process; they sleep between copies).
+namespace {
+
+class HostCopyPool {
+   public:
+    HostCopyPool() {
+        const unsigned hw = std::thread::hardware_concurrency();
+        n_ = std::max(1u, std::min(8u, hw / 2));
+        for (unsigned t = 1; t < n_; ++t) std::thread([this, t] { worker(t); }).detach();
+    }
+    // dst[0, n) = src[0, n), split over the workers and the calling thread.
+    void copy(void *dst, const void *src, size_t n) {
+        constexpr size_t kMinPart = 256 << 10;
+        unsigned parts = (unsigned)std::min<size_t>(n_, std::max<size_t>(1, n / kMinPart));
+        if (parts <= 1) {
+            std::memcpy(dst, src, n);
+            return;
+        }
+        std::lock_guard<std::mutex> one_at_a_time(call_mu_);  // callers on other devices wait here
+        std::unique_lock<std::mutex> lk(mu_);
+        dst_ = static_cast<char *>(dst);
+        src_ = static_cast<const char *>(src);
+        bytes_ = n;
+        parts_ = parts;
+        pending_ = parts - 1;
+        ++gen_;
+        lk.unlock();
+        cv_.notify_all();
+        run_part(0);
+        lk.lock();
+        done_.wait(lk, [this] { return pending_ == 0; });
+    }
+
+   private:
+    void run_part(unsigned t) const {
+        const size_t chunk = (bytes_ + parts_ - 1) / parts_;
+        const size_t b = std::min(bytes_, (size_t)t * chunk), e = std::min(bytes_, b + chunk);
+        if (e > b) std::memcpy(dst_ + b, src_ + b, e - b);
+    }
+    void worker(unsigned t) {
+        unsigned long long seen = 0;
+        std::unique_lock<std::mutex> lk(mu_);
+        while (true) {
+            cv_.wait(lk, [&] { return gen_ != seen; });
+            seen = gen_;
+            if (t >= parts_) continue;
+            lk.unlock();
+            run_part(t);
+            lk.lock();
+            if (--pending_ == 0) done_.notify_one();
+        }
+    }
+    unsigned n_ = 1;
+    std::mutex call_mu_, mu_;
+    std::condition_variable cv_, done_;
+    unsigned long long gen_ = 0;
+    char *dst_ = nullptr;
+    const char *src_ = nullptr;
+    size_t bytes_ = 0;
+    unsigned parts_ = 0, pending_ = 0;
+};
+
+HostCopyPool &host_copy_pool() {
+    static HostCopyPool *pool = new HostCopyPool();  // never destroyed: its threads run until exit
+    return *pool;
+}
+
+bool page_locked(const void *p) {
+    cudaPointerAttributes a{};
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        (void)cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeHost;
+}
+
+}  // namespace
+
+void upload_host_volume(DeviceContext &ctx, const float *src, int nz, int ny, int nx, VolumeArray *arr, float *lin,
+                        cudaStream_t s) {
+    const size_t plane = (size_t)nx * ny * sizeof(float);
+    auto enqueue = [&](const float *from, int z0, int nzc) {
+        if (arr) {
+            cudaMemcpy3DParms p{};
+            p.srcPtr = make_cudaPitchedPtr((void *)from, (size_t)nx * sizeof(float), (size_t)nx, (size_t)ny);
+            p.dstArray = arr->arr;
+            p.dstPos = make_cudaPos(0, 0, (size_t)z0);
+            p.extent = make_cudaExtent((size_t)nx, (size_t)ny, (size_t)nzc);
+            p.kind = cudaMemcpyHostToDevice;
+            DC_CUDA(cudaMemcpy3DAsync(&p, s));
+        } else {
+            DC_CUDA(cudaMemcpyAsync(reinterpret_cast<char *>(lin) + (size_t)z0 * plane, from, (size_t)nzc * plane,
+                                    cudaMemcpyHostToDevice, s));
+        }
+    };
+    if (page_locked(src)) {
+        enqueue(src, 0, nz);
+        return;
+    }
+    constexpr size_t kSlab = 2u << 20;  // bytes per pinned slab (at least one plane)
+    const int zc = (int)std::max<size_t>(1, kSlab / plane);
+    int slot = 0;
+    for (int z0 = 0; z0 < nz; z0 += zc, slot = (slot + 1) % DeviceContext::kStageSlots) {
+        const int n = std::min(zc, nz - z0);
+        // the DMA that last read this slab must be done before it is refilled
+        DC_CUDA(cudaEventSynchronize(ctx.stage_ev[slot]));
+        char *pin = static_cast<char *>(ctx.stage[slot].ensure((size_t)zc * plane));
+        host_copy_pool().copy(pin, reinterpret_cast<const char *>(src) + (size_t)z0 * plane, (size_t)n * plane);
+        enqueue(reinterpret_cast<const float *>(pin), z0, n);
+        DC_CUDA(cudaEventRecord(ctx.stage_ev[slot], s));
+    }
 }
 
 }  // namespace dc

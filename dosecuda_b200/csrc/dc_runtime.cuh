@@ -133,6 +133,12 @@ class DeviceContext {
     PinnedBuffer pin_ring[kPinSlots];
     cudaEvent_t pin_ev[kPinSlots] = {};
     int pin_next = 0;
+    // Ring of pinned slabs for uploading pageable host volumes
+    // (upload_host_volume): a slab is rewritten only after the copy out of it
+    // (event) has completed.
+    static constexpr int kStageSlots = 3;
+    PinnedBuffer stage[kStageSlots];
+    cudaEvent_t stage_ev[kStageSlots] = {};
     cudaEvent_t last_use = nullptr;  // recorded after the last enqueued call
 
     // Orders a call on stream s after every earlier call on this device
@@ -195,6 +201,14 @@ void check_injected_alloc(const char *what);
 // and the whole range must lie inside the one allocation.  Results written
 // this way cross the bus while the kernel runs instead of in a copy after it.
 void *mapped_host_range(const void *host, size_t bytes);
+
+// Host volume (nz, ny, nx floats) -> the cudaArray `arr` or, when `arr` is
+// null, the linear device buffer `lin`, enqueued on s.  A page-locked source
+// is copied directly.  A pageable one is pipelined through the context's
+// pinned slabs: host threads copy slab c into a pinned buffer while the DMA
+// of slab c-1 runs, instead of the driver staging the whole volume serially.
+void upload_host_volume(DeviceContext &ctx, const float *src, int nz, int ny, int nx, VolumeArray *arr, float *lin,
+                        cudaStream_t s);
 
 // Throws Error(DC_ERR_CUDA) if the last launch failed.
 void check_launch(const char *kernel);

@@ -245,11 +245,21 @@ __global__ void __launch_bounds__(128) xray_voxel_kernel(Grid g, Frame f, XrayLa
     } else if (!exact) {
         mt = K;  // short ray: every sample exactly
     }
-    if (exact) {
-        // the whole list is marched exactly by xray_fallback_kernel
-        const unsigned slot = atomicAdd(n_list, 1u);
-        if (DC_IN_BOUNDS(slot, g.n(), 43)) list[slot] = (int)v;
-        return;
+    // Voxels for the exact march go to the list in warp order (one atomic per
+    // warp), so neighbouring rays stay together there and share texture lines.
+    {
+        const unsigned live = __activemask();
+        const unsigned bal = __ballot_sync(live, exact);
+        if (exact) {
+            const int lane = (threadIdx.y * blockDim.x + threadIdx.x) & 31;
+            const int leader = __ffs(bal) - 1;
+            unsigned base = 0;
+            if (lane == leader) base = atomicAdd(n_list, (unsigned)__popc(bal));
+            base = __shfl_sync(bal, base, leader);
+            const unsigned slot = base + __popc(bal & ((1u << lane) - 1u));
+            if (DC_IN_BOUNDS(slot, g.n(), 43)) list[slot] = (int)v;
+            return;
+        }
     }
     float tail = 0.0f;
     for (int t = K - mt; t < K; ++t) tail += march_sample(g, f, density, p, u, (float)t);

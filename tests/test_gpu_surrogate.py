@@ -90,7 +90,7 @@ def test_accepted_beams_pass_gamma_vs_cccs_and_keep_the_mask(setup):
         if accepted:
             accepted_any = True
             assert rate >= 0.99
-            assert _gamma_vs_cccs(engine, maker, dose, ref) >= 0.98
+            assert _gamma_vs_cccs(engine, maker, dose, ref) >= 0.99
             assert torch.all(dose[sur.terma <= 0.01] == 0)
         else:
             assert torch.equal(dose, ref)
