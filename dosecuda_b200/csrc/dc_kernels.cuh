@@ -22,6 +22,7 @@ struct XrayLattice {
     int na, nb, m0, nm;
     float sad;         // source distance (mm)
     float tau;         // largest spread of the four rays' sums interpolated (mm x density)
+    float wet_exact;   // WET (cm) below which a voxel's depth is marched exactly
     float3 src;        // source, image frame relative to the isocentre
     float3 ex, ey, ez; // head-frame axes in the image frame
 };
@@ -31,10 +32,13 @@ bool plan_xray_lattice(const Grid &g, const Frame &f, XrayLattice &L);
 // Photon WET (cm) of every voxel through the lattice, with the reference's
 // march for the voxels the lattice cannot serve (listed in list/n_list, which
 // need room for every voxel); the plain march when the lattice does not apply.
-// `stats` (device word, or null) receives the number of marched voxels
-// (0xffffffff when the lattice did not apply).
+// Voxels whose WET comes out below `wet_exact` (cm) are marched exactly too
+// (+infinity: the plain march for every voxel).  `stats` (device word, or
+// null) receives the number of voxels marched from the list (0xffffffff when
+// the lattice did not apply).
 void launch_xray_depth(DeviceContext &ctx, const Grid &g, const Frame &f, cudaTextureObject_t density, float *wet,
-                       int *list, unsigned *n_list, DeviceBuffer &lattice, unsigned *stats, cudaStream_t s);
+                       int *list, unsigned *n_list, DeviceBuffer &lattice, unsigned *stats, float wet_exact,
+                       cudaStream_t s);
 
 // ---- proton pencil beam (dc_proton.cu) -----------------------------------
 // One energy layer: a run of spots with the same energy id

@@ -234,7 +234,7 @@ __device__ __forceinline__ float cccs_voxel(const Grid &g, const Frame &f, const
                                             const float4 *s_dir, const float *s_rl10, cudaTextureObject_t td_tex,
                                             float3 p);
 
-__global__ void __launch_bounds__(128, 10) cccs_kernel(Grid g, Frame f, CccsCones C, float sp_cm, float dose_scale,
+__global__ void __launch_bounds__(128) cccs_kernel(Grid g, Frame f, CccsCones C, float sp_cm, float dose_scale,
                                                    const float4 *__restrict__ dirs, cudaTextureObject_t td_tex,
                                                    const float *__restrict__ electron, const int *__restrict__ active,
                                                    const unsigned *__restrict__ n_active, float *__restrict__ dose) {
@@ -461,12 +461,24 @@ static unsigned cccs_blocks(const DeviceContext &ctx, long long work) {
 
 DC_BOUNDS_TAKE(take_bounds_photon)
 
+// WET (cm) below which the electron contamination term of terma_kernel is
+// non-zero, plus a margin well above the lattice's interpolation error
+// (0.03 cm): max(0, (e^{-ea w} - e^{-ea efd}) / (1 - e^{-ea efd})) vanishes
+// for w >= efd when ea > 0 and efd > 0.  Without an electron term there is no
+// bound (-inf); with parameters that keep it non-zero at every depth the
+// lattice is not used at all (+inf).
+static float electron_exact_wet(const PhotonParams &P) {
+    if (P.esw == 0.0f) return -INFINITY;
+    if (P.ea > 0.0f && P.efd > 0.0f && P.efd < 1.0e4f) return P.efd + 0.1f;
+    return INFINITY;
+}
+
 void enqueue_terma(DeviceContext &ctx, const Grid &g, const Frame &f, const PhotonParams &P, const CccsCones &C,
                    const PhotonWork &w, float *dose_dev, float *terma_out, cudaStream_t s) {
     if (g.n() > 0x7fffffffLL) throw Error(DC_ERR_VALUE, "photon volumes are limited to 2^31 - 1 voxels.");
     if (w.depth_mode == 1 && w.xlat != nullptr)
         launch_xray_depth(ctx, g, f, w.dens_tex, w.wet, w.active, w.n_active, *w.xlat, w.depth_stats,
-                          s);  // the active list is free until the TERMA kernel fills it
+                          electron_exact_wet(P), s);  // the active list is free until the TERMA kernel fills it
     else {
         launch_wet_march(ctx, g, f, w.dens_tex, w.wet, s);
         if (w.depth_stats != nullptr) DC_CUDA(cudaMemsetAsync(w.depth_stats, 0xff, sizeof(unsigned), s));

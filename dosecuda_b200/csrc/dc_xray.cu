@@ -39,8 +39,13 @@
 // one lattice cell is second order; where the four rays disagree by more than
 // tau the exact march runs, so a voxel's interpolated sum can never be off by
 // more than tau.  With tau = 0.3 mm of unit density the photon WET stays
-// within 0.03 cm of the march, i.e. TERMA within ~0.15 % at 6 MV.  The proton
-// WET never uses this path: there the march is kept bit-exact.
+// within 0.03 cm of the march, i.e. TERMA within ~0.15 % at 6 MV.  The
+// electron contamination term is far steeper in WET (its slope at the surface
+// is ~1 per cm of WET: 0.03 cm would move a surface voxel's dose by ~3 % of
+// the maximum), and it is non-zero only above its fitted depth efd, so every
+// voxel whose interpolated WET is below efd + 0.1 cm is marched exactly
+// (inline when its ray is short).  The proton WET never uses this path: there
+// the march is kept bit-exact.
 #include <algorithm>
 #include <cmath>
 
@@ -56,6 +61,7 @@ namespace {
 
 constexpr int kRaysPerBlock = 32;  // rays of one lattice row per block, one warp each
 constexpr int kMaxTail = 32;       // exact boundary samples before the whole march is taken instead
+constexpr int kInlineMarch = 64;   // longest ray a shallow voxel marches inline instead of joining the list
 
 __device__ __forceinline__ bool march_inside(const Grid &g, const Frame &f, float3 p, float3 u, float t) {
     float3 q;
@@ -245,6 +251,25 @@ __global__ void __launch_bounds__(128) xray_voxel_kernel(Grid g, Frame f, XrayLa
     } else if (!exact) {
         mt = K;  // short ray: every sample exactly
     }
+    if (!exact) {
+        if (mt == K) {
+            wet_sum = march_from(g, f, density, p, u, 0.0f, -0.05f);  // the reference's own sum
+        } else {
+            float tail = 0.0f;
+            for (int t = K - mt; t < K; ++t) tail += march_sample(g, f, density, p, u, (float)t);
+            wet_sum = fmaf(S + tail, 0.1f, -0.05f);
+            // Shallow voxels: the electron contamination term falls by ~1 % of
+            // its value per 0.01 cm of WET there, far steeper than TERMA, so
+            // their depth is marched exactly (short rays, inline; long ones,
+            // e.g. through air, join the list).
+            if (!(wet_sum >= L.wet_exact)) {
+                if (K <= kInlineMarch)
+                    wet_sum = march_from(g, f, density, p, u, 0.0f, -0.05f);
+                else
+                    exact = true;
+            }
+        }
+    }
     // Voxels for the exact march go to the list in warp order (one atomic per
     // warp), so neighbouring rays stay together there and share texture lines.
     {
@@ -261,9 +286,6 @@ __global__ void __launch_bounds__(128) xray_voxel_kernel(Grid g, Frame f, XrayLa
             return;
         }
     }
-    float tail = 0.0f;
-    for (int t = K - mt; t < K; ++t) tail += march_sample(g, f, density, p, u, (float)t);
-    wet_sum = fmaf(S + tail, 0.1f, -0.05f);
     if (DC_IN_BOUNDS(v, g.n(), 44)) wet[v] = wet_sum;
 }
 
@@ -342,13 +364,15 @@ bool plan_xray_lattice(const Grid &g, const Frame &f, XrayLattice &L) {
 }
 
 void launch_xray_depth(DeviceContext &ctx, const Grid &g, const Frame &f, cudaTextureObject_t density, float *wet,
-                       int *list, unsigned *n_list, DeviceBuffer &lattice, unsigned *stats, cudaStream_t s) {
+                       int *list, unsigned *n_list, DeviceBuffer &lattice, unsigned *stats, float wet_exact,
+                       cudaStream_t s) {
     XrayLattice L;
-    if (!plan_xray_lattice(g, f, L)) {
+    if (!(wet_exact < INFINITY) || !plan_xray_lattice(g, f, L)) {
         launch_wet_march(ctx, g, f, density, wet, s);
         if (stats != nullptr) DC_CUDA(cudaMemsetAsync(stats, 0xff, sizeof(unsigned), s));  // all voxels marched
         return;
     }
+    L.wet_exact = wet_exact;
     float *G = static_cast<float *>(lattice.ensure((size_t)L.na * L.nb * L.nm * sizeof(float)));
     {
         KernelTimer kt(ctx, "xray_lattice", s);

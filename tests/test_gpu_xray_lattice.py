@@ -7,7 +7,11 @@ oracle.
 The lattice interpolates each voxel's density integral from the four lattice
 rays around its ray and marches exactly wherever they disagree by more than
 0.3 mm of unit density (0.03 cm of WET), so TERMA may move by at most the
-attenuation of 0.03 cm of water; the dose is held to the parity bar."""
+attenuation of 0.03 cm of water; voxels shallower than the electron
+contamination term's fitted depth (plus 0.1 cm) are marched exactly, since
+that term changes by ~1 % per 0.01 cm of WET.  The dose is held to the parity
+bar; the fully open 40 x 40 cm field puts the whole entry face, every side
+face and the electron term's whole depth range in the beam."""
 import glob
 import os
 import sys
@@ -23,6 +27,7 @@ pytestmark = pytest.mark.gpu
 GEOMETRIES = {
     # name: (phantom kwargs, plan kwargs)
     "small_photon_128": ({}, {}),
+    "open_field_128": ({}, {"field_cm": (40.0, 40.0)}),
     "gantry30_coll20": ({"shape": (96, 96, 96), "spacing": 3.0, "seed": 4}, {"gantry": 30.0, "collimator": 20.0,
                                                                              "field_cm": (8.0, 12.0)}),
     "gantry250_couch30": ({"shape": (80, 96, 72), "spacing": 3.5, "seed": 5}, {"gantry": 250.0, "couch": 30.0,
