@@ -454,6 +454,30 @@ def run_batched(args, local, dist_mod, ws):
             dose_kernels.proton_spot_cuda(model, vol, wv, bm, local)
             bi += 1
     t_calls = aggregate_max((time.perf_counter() - t0) * 1e3, dist_mod)
+    # influence matrices (CSR, cutoff 1e-4 of each spot's maximum), beam by
+    # beam, count then fill: one beam's matrix is alive at a time
+    csr = None
+    if args.batch_csr:
+        b.influence_csr(0, cutoff=1e-4)  # warm-up (kernel attributes, allocator)
+        torch.cuda.synchronize()
+        nnz_tot, max_bytes, bytes_tot = 0, 0, 0
+        t0 = time.perf_counter()
+        for bid in range(b.n_beams):
+            r, c, v = b.influence_csr(bid, cutoff=1e-4)
+            nnz = c.numel()
+            nnz_tot += nnz
+            bytes_tot += r.numel() * 8 + nnz * 8
+            max_bytes = max(max_bytes, r.numel() * 8 + nnz * 8)
+            del r, c, v
+        torch.cuda.synchronize()
+        t_csr = aggregate_max((time.perf_counter() - t0) * 1e3, dist_mod)
+        csr = {"ms_all_beams": round(t_csr, 2), "beams": b.n_beams, "nnz_total": int(nnz_tot),
+               "entries_per_s": round(nnz_tot / (t_csr * 1e-3), 1),
+               "gb_written": round(bytes_tot / 1e9, 3),
+               "max_beam_gb": round(max_bytes / 1e9, 3),
+               "what": "per beam: spot-max, count, scan, fill passes; float32 values, int32 spot columns, int64 "
+                       "voxel row starts; entries >= 1e-4 x the spot's maximum; wall clock including the "
+                       "count's host read and the arrays' allocation"}
     n_spots = b.n_spots
     out = {
         "metric": "batched IMPT dose: ms per optimisation iteration (all plans)",
@@ -463,6 +487,7 @@ def run_batched(args, local, dist_mod, ws):
         "per_plan_calls_ms": round(t_calls, 3),
         "speedup_vs_per_plan_calls": round(t_calls / t_batch, 2),
         "tile_variant": int(variant), "tile_ms": [round(x, 3) for x in getattr(b, "tune_ms", [])],
+        "influence_csr": csr,
         "config": {"workload": "%d plans x 256x256x160 @ 1.5x1.5x2.0 mm, %d beams, %d spots; body ellipsoid "
                                "(20+-40 HU) with bone/lung/air ellipsoids, spherical target, layers at 3 mm R80 "
                                "spacing, 4-6 mm spot grid, lognormal(0, 0.5) weights" %
@@ -1087,6 +1112,8 @@ def main():
     ap.add_argument("--impl", default="mine", choices=["mine", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU oracle baseline")
     ap.add_argument("--batch-plans", type=int, default=16, help="plans in the batched workload (0: skip)")
+    ap.add_argument("--no-batch-csr", dest="batch_csr", action="store_false",
+                    help="skip the batched workload's influence matrices")
     ap.add_argument("--opt-iters", type=int, default=200, help="optimisation iterations (0: skip)")
     ap.add_argument("--tune-cache", action="store_true", help="keep the tile autotuner's JSON cache")
     ap.add_argument("--surrogate-beams", type=int, default=300, help="held-out beams for the surrogate (0: skip)")

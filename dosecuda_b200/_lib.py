@@ -132,6 +132,10 @@ SIGNATURES = {
     "dc_proton_batch_beam_spot_offset": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int)]),
     "dc_proton_batch_wet": (C.c_int, [C.c_void_p, C.c_void_p]),
     "dc_proton_batch_dose": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]),
+    "dc_proton_batch_influence_count": (C.c_int, [C.c_void_p, C.c_int, C.c_float, C.c_void_p,
+                                                  C.POINTER(C.c_longlong), C.c_void_p]),
+    "dc_proton_batch_influence_fill": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
+                                                 C.c_longlong, C.c_void_p]),
     "dc_proton_batch_destroy": (C.c_int, [C.c_void_p]),
     "dc_photon_dose": (C.c_int, _VOL + [C.POINTER(PhotonModel), C.POINTER(ControlPoint), C.c_void_p]),
     "dc_photon_dose_dev": (C.c_int, _VOL + [C.POINTER(PhotonModel), C.POINTER(ControlPoint), C.c_void_p,

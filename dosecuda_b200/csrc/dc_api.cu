@@ -396,6 +396,7 @@ int dc_photon_dose(int gpu_id, const float *density, int nz, int ny, int nx, con
         const Grid g = make_grid(nz, ny, nx, spacing);
         const Frame f = make_frame(cp->iso, origin, cp->gantry_deg, cp->couch_deg, cp->collimator_deg,
                                    model->primary_source_distance);
+        photon_head_fork(ctx, g, f, P, s);  // the head factors need no density: they run during the upload
         ctx.density.ensure(nx, ny, nz, false);
         upload_host_volume(ctx, density, nz, ny, nx, &ctx.density, nullptr, s);
         const size_t vb = (size_t)g.n() * sizeof(float);

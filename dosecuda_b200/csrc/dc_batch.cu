@@ -69,6 +69,13 @@ struct dc_proton_batch {
     DeviceBuffer queue;     // unsigned queue head
     DeviceBuffer wet_raw;   // unsmoothed WET scratch (largest plan)
     std::vector<std::unique_ptr<VolumeArray>> arrays;  // per-plan RLSP texture
+    std::vector<PbBatchBeam> hbeams;  // host copies of d_beams (beams grouped by plan)
+    // influence-matrix scratch, one beam at a time: spot maxima, thresholds,
+    // per-voxel counts, scan block sums; `inf_beam` is the beam (add order)
+    // whose thresholds they hold and `inf_nnz` its entry count
+    DeviceBuffer inf_spot_max, inf_thr, inf_counts, inf_sums;
+    int inf_beam = -1;
+    long long inf_nnz = 0;
 
     ~dc_proton_batch() {
         luts.release();
@@ -80,6 +87,10 @@ struct dc_proton_batch {
         queue.release();
         wet_raw.release();
         for (auto &a : arrays) a->release();
+        inf_spot_max.release();
+        inf_thr.release();
+        inf_counts.release();
+        inf_sums.release();
     }
 };
 
@@ -90,6 +101,19 @@ void need(bool ok, const std::string &m) {
 }
 
 size_t align256(size_t n) { return (n + 255) & ~(size_t)255; }
+
+// Position of beam `beam_id` (add order) among the committed beams, which
+// are grouped by plan.
+int committed_index(const dc_proton_batch *b, int beam_id) {
+    need(beam_id >= 0 && beam_id < (int)b->beams.size(), "unknown beam id.");
+    int seen = 0;
+    for (auto &p : b->plans)
+        for (int id : p.beams) {
+            if (id == beam_id) return seen;
+            ++seen;
+        }
+    throw Error(DC_ERR_VALUE, "unknown beam id.");
+}
 
 }  // namespace
 
@@ -241,6 +265,7 @@ int dc_proton_batch_commit(dc_proton_batch *b) {
         DC_CUDA(cudaMemcpy(dp, hplans.data(), hplans.size() * sizeof(PbBatchPlan), cudaMemcpyHostToDevice));
         void *db = b->d_beams.ensure(hbeams.size() * sizeof(PbBatchBeam));
         DC_CUDA(cudaMemcpy(db, hbeams.data(), hbeams.size() * sizeof(PbBatchBeam), cudaMemcpyHostToDevice));
+        b->hbeams = hbeams;
         // work queues, one per tile shape: plans by decreasing cost, tiles in order
         std::vector<int> plan_order(b->plans.size());
         std::iota(plan_order.begin(), plan_order.end(), 0);
@@ -289,18 +314,8 @@ int dc_proton_batch_info(const dc_proton_batch *b, int *n_plans, int *n_beams, i
 int dc_proton_batch_beam_spot_offset(const dc_proton_batch *b, int beam_id, int *offset) {
     return guarded([&] {
         need(b != nullptr && b->committed, "batch handle must be committed.");
-        need(beam_id >= 0 && beam_id < (int)b->beams.size() && offset, "unknown beam id.");
-        // beam ids are in add order; after commit beams are grouped by plan
-        int seen = 0;
-        for (auto &p : b->plans)
-            for (int id : p.beams) {
-                if (id == beam_id) {
-                    *offset = b->beams[seen].spot_base;
-                    return;
-                }
-                ++seen;
-            }
-        throw Error(DC_ERR_VALUE, "unknown beam id.");
+        need(offset != nullptr, "NULL argument.");
+        *offset = b->beams[committed_index(b, beam_id)].spot_base;
     });
 }
 
@@ -346,6 +361,58 @@ int dc_proton_batch_dose(dc_proton_batch *b, const float *mu_dev, int variant, v
         launch_pencil_beam_batch(ctx, variant, b->d_plans.as<const PbBatchPlan>(), b->d_beams.as<const PbBatchBeam>(),
                                  b->d_items[variant].as<const int2>(), b->n_items[variant], b->queue.as<unsigned>(),
                                  b->lut_len, s);
+        ctx.end_call(s);
+    });
+}
+
+int dc_proton_batch_influence_count(dc_proton_batch *b, int beam_id, float cutoff, long long *row_ptr_dev,
+                                    long long *nnz, void *stream) {
+    return guarded([&] {
+        need(b != nullptr && b->committed, "batch handle must be committed.");
+        need(row_ptr_dev != nullptr && nnz != nullptr, "NULL argument.");
+        need(std::isfinite(cutoff) && cutoff >= 0.0f && cutoff < 1.0f, "'cutoff' must be in [0, 1).");
+        const int bi = committed_index(b, beam_id);
+        DeviceContext &ctx = context(b->device);
+        std::lock_guard<std::mutex> lk(ctx.mu);
+        cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+        const HostBeam &hb = b->beams[bi];
+        const Grid &g = b->plans[hb.plan].g;
+        const int n_spots = (int)hb.spots.size();
+        b->inf_beam = -1;
+        ctx.begin_call(s);
+        unsigned *sm = static_cast<unsigned *>(b->inf_spot_max.ensure((size_t)std::max(n_spots, 1) * sizeof(unsigned)));
+        float *thr = static_cast<float *>(b->inf_thr.ensure((size_t)std::max(n_spots, 1) * sizeof(float)));
+        int *counts = static_cast<int *>(b->inf_counts.ensure((size_t)g.n() * sizeof(int)));
+        launch_influence_count(ctx, g, hb.f, b->hbeams[bi].t, n_spots, hb.wet, cutoff, sm, thr, counts, s);
+        launch_scan_counts(counts, g.n(), row_ptr_dev, b->inf_sums, s);
+        DC_CUDA(cudaMemcpyAsync(nnz, row_ptr_dev + g.n(), sizeof(long long), cudaMemcpyDeviceToHost, s));
+        ctx.end_call(s);
+        DC_CUDA(cudaStreamSynchronize(s));
+        b->inf_beam = beam_id;
+        b->inf_nnz = *nnz;
+    });
+}
+
+int dc_proton_batch_influence_fill(dc_proton_batch *b, int beam_id, const long long *row_ptr_dev, int *col_dev,
+                                   float *val_dev, long long capacity, void *stream) {
+    return guarded([&] {
+        need(b != nullptr && b->committed, "batch handle must be committed.");
+        need(row_ptr_dev != nullptr && col_dev != nullptr && val_dev != nullptr, "NULL device buffer.");
+        const int bi = committed_index(b, beam_id);
+        need(b->inf_beam == beam_id, "dc_proton_batch_influence_count must run for this beam first.");
+        need(capacity >= b->inf_nnz, "'capacity' is below the beam's entry count.");
+        DeviceContext &ctx = context(b->device);
+        std::lock_guard<std::mutex> lk(ctx.mu);
+        cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+        const HostBeam &hb = b->beams[bi];
+        ctx.begin_call(s);
+        PbExtra x;
+        x.cap = capacity;
+        x.thr = b->inf_thr.as<const float>();
+        x.row_ptr = row_ptr_dev;
+        x.col = col_dev;
+        x.val = val_dev;
+        launch_pencil_beam_mode(ctx, kPbFill, b->plans[hb.plan].g, hb.f, b->hbeams[bi].t, hb.wet, x, s);
         ctx.end_call(s);
     });
 }

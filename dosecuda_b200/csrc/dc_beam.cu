@@ -133,16 +133,43 @@ __global__ void spot_thr_kernel(const unsigned *__restrict__ spot_max, float cut
     if (s < n) thr[s] = cutoff * __uint_as_float(spot_max[s]);
 }
 
-// counts -> row_ptr (n_vox + 1 entries) on stream s
-void scan_counts(dc_proton_beam *b, long long *row_ptr, cudaStream_t s) {
-    const int nb = (int)((b->n_vox + kScanBlock - 1) / kScanBlock);
-    long long *sums = static_cast<long long *>(b->block_sums.ensure(((size_t)nb + 1) * sizeof(long long)));
-    scan_blocks_kernel<<<nb, kScanBlock, 0, s>>>(b->counts.as<int>(), b->n_vox, row_ptr, sums);
+}  // namespace
+
+namespace dc {
+
+void launch_scan_counts(const int *counts, long long n, long long *row_ptr, DeviceBuffer &scratch, cudaStream_t s) {
+    const int nb = (int)((n + kScanBlock - 1) / kScanBlock);
+    long long *sums = static_cast<long long *>(scratch.ensure(((size_t)nb + 1) * sizeof(long long)));
+    scan_blocks_kernel<<<nb, kScanBlock, 0, s>>>(counts, n, row_ptr, sums);
     check_launch("scan_blocks_kernel");
     scan_sums_kernel<<<1, kScanBlock, 0, s>>>(sums, nb);
     check_launch("scan_sums_kernel");
-    scan_add_kernel<<<nb, kScanBlock, 0, s>>>(row_ptr, b->n_vox, sums, nb);
+    scan_add_kernel<<<nb, kScanBlock, 0, s>>>(row_ptr, n, sums, nb);
     check_launch("scan_add_kernel");
+}
+
+void launch_influence_count(DeviceContext &ctx, const Grid &g, const Frame &f, const ProtonTables &t, int n_spots,
+                            const float *wet, float cutoff, unsigned *spot_max, float *thr, int *counts,
+                            cudaStream_t s) {
+    DC_CUDA(cudaMemsetAsync(spot_max, 0, (size_t)n_spots * sizeof(unsigned), s));
+    PbExtra x;
+    x.spot_max = spot_max;
+    launch_pencil_beam_mode(ctx, kPbSpotMax, g, f, t, wet, x, s);
+    spot_thr_kernel<<<(n_spots + 255) / 256, 256, 0, s>>>(spot_max, cutoff, thr, n_spots);
+    check_launch("spot_thr_kernel");
+    PbExtra y;
+    y.thr = thr;
+    y.counts = counts;
+    launch_pencil_beam_mode(ctx, kPbCount, g, f, t, wet, y, s);
+}
+
+}  // namespace dc
+
+namespace {
+
+// counts -> row_ptr (n_vox + 1 entries) on stream s
+void scan_counts(dc_proton_beam *b, long long *row_ptr, cudaStream_t s) {
+    launch_scan_counts(b->counts.as<int>(), b->n_vox, row_ptr, b->block_sums, s);
 }
 
 // spot maxima -> thresholds -> per-voxel counts, on stream s
@@ -150,16 +177,7 @@ void count_pass(DeviceContext &ctx, dc_proton_beam *b, const float *wet, float c
     unsigned *sm = static_cast<unsigned *>(b->spot_max.ensure((size_t)b->n_spots * sizeof(unsigned)));
     float *thr = static_cast<float *>(b->thr.ensure((size_t)b->n_spots * sizeof(float)));
     int *counts = static_cast<int *>(b->counts.ensure((size_t)b->n_vox * sizeof(int)));
-    DC_CUDA(cudaMemsetAsync(sm, 0, (size_t)b->n_spots * sizeof(unsigned), s));
-    PbExtra x;
-    x.spot_max = sm;
-    launch_pencil_beam_mode(ctx, kPbSpotMax, b->g, b->f, b->view(), wet, x, s);
-    spot_thr_kernel<<<(b->n_spots + 255) / 256, 256, 0, s>>>(sm, cutoff, thr, b->n_spots);
-    check_launch("spot_thr_kernel");
-    PbExtra y;
-    y.thr = thr;
-    y.counts = counts;
-    launch_pencil_beam_mode(ctx, kPbCount, b->g, b->f, b->view(), wet, y, s);
+    launch_influence_count(ctx, b->g, b->f, b->view(), b->n_spots, wet, cutoff, sm, thr, counts, s);
 }
 
 DeviceContext &beam_ctx(dc_proton_beam *b) {

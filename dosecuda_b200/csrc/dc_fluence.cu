@@ -83,6 +83,7 @@ __global__ void __launch_bounds__(128) fluence_modulate_kernel(Grid g, Frame f, 
     float wa, wb;
     fluence_taps(M, f, voxel_xyz(g, f, i, j, k), idx, w, &wa, &wb);
     const int nmap = M.na * M.nb;
+    (void)nmap;  // read by the bounds checks of debug builds
     float fv[4];
 #pragma unroll
     for (int q = 0; q < 4; ++q) fv[q] = DC_IN_BOUNDS(idx[q], nmap, 50) ? __ldg(F + idx[q]) : 0.0f;
@@ -204,6 +205,7 @@ __global__ void __launch_bounds__(128) fluence_grad_kernel(Grid g, Frame f, Flue
                                                            double *__restrict__ grad_F) {
     extern __shared__ double s_acc[];
     const int nmap = M.na * M.nb;
+    (void)nmap;  // read by the bounds checks of debug builds
     const bool in_smem = nmap <= kMaxSmemBeamlets;
     const int tid = threadIdx.y * blockDim.x + threadIdx.x;
     if (in_smem)
@@ -274,6 +276,7 @@ void enqueue_fluence_adjoint(DeviceContext &ctx, const Grid &g, const Frame &f, 
     {
         KernelTimer kt(ctx, "fluence_grad", s);
         const int nmap = M.na * M.nb;
+    (void)nmap;  // read by the bounds checks of debug builds
         const size_t smem = nmap <= kMaxSmemBeamlets ? (size_t)nmap * sizeof(double) : 0;
         fluence_grad_kernel<<<fl_grid(g), dim3(32, 4, 1), smem, s>>>(g, f, M, dose_scale, T0, E0, h, grad_dose, grad_F);
         check_launch("fluence_grad_kernel");

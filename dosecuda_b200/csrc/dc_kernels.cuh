@@ -127,6 +127,17 @@ void launch_pencil_beam_list(DeviceContext &ctx, int mode, const Grid &g, const 
 void launch_pencil_beam_mode(DeviceContext &ctx, int mode, const Grid &g, const Frame &f, const ProtonTables &t,
                              const float *wet_s, const PbExtra &x, cudaStream_t s);
 
+// ---- dose-influence matrix, count-then-fill (dc_beam.cu) -------------------
+// Count pass of one beam: spot_max[s] = max_v K_s(v) (float bits), thr[s] =
+// cutoff * spot_max[s], counts[v] = #{s : K_s(v) >= thr[s]}.  The fill pass is
+// launch_pencil_beam_mode(kPbFill) with the same thresholds and the row starts.
+void launch_influence_count(DeviceContext &ctx, const Grid &g, const Frame &f, const ProtonTables &t, int n_spots,
+                            const float *wet, float cutoff, unsigned *spot_max, float *thr, int *counts,
+                            cudaStream_t s);
+// Exclusive scan of n int counts into n + 1 int64 row starts (row_ptr[n] =
+// the total); `scratch` grows to ceil(n / 1024) + 1 int64 block sums.
+void launch_scan_counts(const int *counts, long long n, long long *row_ptr, DeviceBuffer &scratch, cudaStream_t s);
+
 // ---- batched pencil beam (persistent, many plans) -------------------------
 struct PbBatchBeam {
     Frame f;

@@ -125,19 +125,13 @@ __device__ __forceinline__ float head_transmission(const PhotonParams &P, float3
     return trans;
 }
 
-// Writes (TERMA, density) of each voxel as one float2 texel of the CCCS
-// volume; the density is the input texture read at the texel centre, where
-// linear filtering returns the stored value unchanged.  It also applies the
-// CCCS mask (dose 0 where TERMA <= 0.01, IMRTClasses.cu:270-273): masked
-// voxels get their zero dose here, the others are appended to `active`
-// (warp-aggregated), so the CCCS runs on full warps of active voxels only.
-// dose (or null) receives the zero of masked voxels; terma_out (or null) a
-// linear copy of the TERMA volume.
-__global__ void __launch_bounds__(128) terma_kernel(Grid g, Frame f, PhotonParams P, const float *__restrict__ wet,
-                                                    cudaTextureObject_t dens_tex, cudaSurfaceObject_t td_surf,
-                                                    float *__restrict__ electron,
-                                                    float *__restrict__ dose, float *__restrict__ terma_out,
-                                                    int *__restrict__ active, unsigned *__restrict__ n_active) {
+// Head factors of each voxel, which do not depend on the density: the
+// primary and scatter transmission through the collimator
+// (headTransmission, IMRTClasses.cu:120-150) and the off-axis intensity and
+// softening (offAxisFactors, IMRTClasses.cu:152-171), as (tp, ts, oaf, soft).
+// Split from the TERMA kernel so that it can run on a side stream while the
+// density is uploaded or the radiological depth is traced.
+__global__ void __launch_bounds__(128) head_kernel(Grid g, Frame f, PhotonParams P, float4 *__restrict__ head) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
     const int k = blockIdx.z;
@@ -146,11 +140,6 @@ __global__ void __launch_bounds__(128) terma_kernel(Grid g, Frame f, PhotonParam
 
     const float3 p = voxel_xyz(g, f, i, j, k);
     const float3 h = image_to_head<true>(f, p);
-
-    const float d_primary = P.psd - h.z;
-    const float d_scatter = P.ssd - h.z;
-
-    // offAxisFactors (IMRTClasses.cu:152-171)
     const float d_src = P.psd - h.z;
     const float r_cax = hypotf(h.x, h.y) * d_src / P.psd;
     float oaf, soft;
@@ -171,6 +160,36 @@ __global__ void __launch_bounds__(128) terma_kernel(Grid g, Frame f, PhotonParam
     }
     const float tp = head_transmission(P, h, P.psd, P.pss);
     const float ts = head_transmission(P, h, P.ssd, P.sss);
+    if (DC_IN_BOUNDS(v, g.n(), 11)) head[v] = make_float4(tp, ts, oaf, soft);
+}
+
+// Writes (TERMA, density) of each voxel as one float2 texel of the CCCS
+// volume; the density is the input texture read at the texel centre, where
+// linear filtering returns the stored value unchanged.  It also applies the
+// CCCS mask (dose 0 where TERMA <= 0.01, IMRTClasses.cu:270-273): masked
+// voxels get their zero dose here, the others are appended to `active`
+// (warp-aggregated), so the CCCS runs on full warps of active voxels only.
+// dose (or null) receives the zero of masked voxels; terma_out (or null) a
+// linear copy of the TERMA volume.  `head` holds head_kernel's factors.
+__global__ void __launch_bounds__(128) terma_kernel(Grid g, Frame f, PhotonParams P, const float *__restrict__ wet,
+                                                    const float4 *__restrict__ head,
+                                                    cudaTextureObject_t dens_tex, cudaSurfaceObject_t td_surf,
+                                                    float *__restrict__ electron,
+                                                    float *__restrict__ dose, float *__restrict__ terma_out,
+                                                    int *__restrict__ active, unsigned *__restrict__ n_active) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int k = blockIdx.z;
+    if (i >= g.nx || j >= g.ny) return;
+    const long long v = (long long)i + (long long)g.nx * (j + (long long)g.ny * k);
+    const bool v_ok = DC_IN_BOUNDS(v, g.n(), 10);
+
+    const float3 p = voxel_xyz(g, f, i, j, k);
+    const float3 h = image_to_head<true>(f, p);
+    const float d_primary = P.psd - h.z;
+    const float d_scatter = P.ssd - h.z;
+    const float4 hf = v_ok ? __ldg(head + v) : make_float4(0.f, 0.f, 0.f, 0.f);
+    const float tp = hf.x, ts = hf.y, oaf = hf.z, soft = hf.w;
     const float w = __ldg(wet + v);
     const float ratio = fminf(1.00f, ts / tp);
     const float geo_p = sqr(P.psd / d_primary);
@@ -185,7 +204,6 @@ __global__ void __launch_bounds__(128) terma_kernel(Grid g, Frame f, PhotonParam
     const float T = oaf * ((1.0f - P.ssw) * tp * terma + P.ssw * ts * terma);
     const float rho = tex3D<float>(dens_tex, (float)i + 0.5f, (float)j + 0.5f, (float)k + 0.5f);
     surf3Dwrite(make_float2(T, rho), td_surf, i * (int)sizeof(float2), j, k);
-    const bool v_ok = DC_IN_BOUNDS(v, g.n(), 10);
     if (v_ok) electron[v] = P.esw * (0.4f + (0.3f * ratio)) * elec * tp;
     if (terma_out && v_ok) terma_out[v] = T;
 
@@ -473,9 +491,24 @@ static float electron_exact_wet(const PhotonParams &P) {
     return INFINITY;
 }
 
+void photon_head_fork(DeviceContext &ctx, const Grid &g, const Frame &f, const PhotonParams &P, cudaStream_t s) {
+    float4 *head = static_cast<float4 *>(ctx.head.ensure((size_t)g.n() * sizeof(float4)));
+    DC_CUDA(cudaEventRecord(ctx.fork_ev, s));
+    DC_CUDA(cudaStreamWaitEvent(ctx.side, ctx.fork_ev, 0));
+    {
+        KernelTimer kt(ctx, "head", ctx.side);
+        head_kernel<<<vol_grid(g), dim3(32, 4, 1), 0, ctx.side>>>(g, f, P, head);
+        check_launch("head_kernel");
+    }
+    DC_CUDA(cudaEventRecord(ctx.join_ev, ctx.side));
+    ctx.head_forked = true;
+}
+
 void enqueue_terma(DeviceContext &ctx, const Grid &g, const Frame &f, const PhotonParams &P, const CccsCones &C,
                    const PhotonWork &w, float *dose_dev, float *terma_out, cudaStream_t s) {
     if (g.n() > 0x7fffffffLL) throw Error(DC_ERR_VALUE, "photon volumes are limited to 2^31 - 1 voxels.");
+    // the head factors run beside the depth pass unless the caller forked them earlier
+    if (!ctx.head_forked) photon_head_fork(ctx, g, f, P, s);
     if (w.depth_mode == 1 && w.xlat != nullptr)
         launch_xray_depth(ctx, g, f, w.dens_tex, w.wet, w.active, w.n_active, *w.xlat, w.depth_stats,
                           electron_exact_wet(P), s);  // the active list is free until the TERMA kernel fills it
@@ -484,10 +517,13 @@ void enqueue_terma(DeviceContext &ctx, const Grid &g, const Frame &f, const Phot
         if (w.depth_stats != nullptr) DC_CUDA(cudaMemsetAsync(w.depth_stats, 0xff, sizeof(unsigned), s));
     }
     DC_CUDA(cudaMemsetAsync(w.n_active, 0, sizeof(unsigned), s));
+    DC_CUDA(cudaStreamWaitEvent(s, ctx.join_ev, 0));
+    ctx.head_forked = false;
     {
         KernelTimer kt(ctx, "terma", s);
-        terma_kernel<<<vol_grid(g), dim3(32, 4, 1), 0, s>>>(g, f, P, w.wet, w.dens_tex, w.td_surf, w.electron,
-                                                            dose_dev, terma_out, w.active, w.n_active);
+        terma_kernel<<<vol_grid(g), dim3(32, 4, 1), 0, s>>>(g, f, P, w.wet, ctx.head.as<const float4>(), w.dens_tex,
+                                                            w.td_surf, w.electron, dose_dev, terma_out, w.active,
+                                                            w.n_active);
         check_launch("terma_kernel");
     }
     cone_dirs_kernel<<<1, kMaxCones * 12, 0, s>>>(f, C, w.dirs);

@@ -60,6 +60,11 @@ struct PhotonWork {
     int depth_mode = 1;                // 0: per-voxel march, 1: ray lattice (DeviceContext::photon_depth_mode)
 };
 
+// Enqueues the density-independent head factors of every voxel (collimator
+// transmission, off-axis factors) on the context's side stream, after the
+// work enqueued on s so far.  The next enqueue_terma joins it; without this
+// call enqueue_terma forks it itself, beside the depth pass.
+void photon_head_fork(DeviceContext &ctx, const Grid &g, const Frame &f, const PhotonParams &P, cudaStream_t s);
 // Ray trace + TERMA + cone directions.  dose_dev (or null) receives the zero
 // of every masked voxel, terma_out (or null) a linear TERMA copy.
 void enqueue_terma(DeviceContext &ctx, const Grid &g, const Frame &f, const PhotonParams &P, const CccsCones &C,

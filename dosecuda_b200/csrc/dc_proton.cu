@@ -261,6 +261,12 @@ void launch_layer_rcut(const Grid &g, const Frame &f, LayerRec *layers, int n_la
 //   kPbSpotMax  spot_max[s]   = max_v K_s(v)
 //   kPbCount    counts[v]     = #{s : K_s(v) >= thr[s]}
 //   kPbFill     CSR row v     = (s, K_s(v)) for K_s(v) >= thr[s], in spot-table order
+//               (run by the kPbCount instantiation with x.row_ptr set: the
+//               fill must take exactly the pairs the count took, so both
+//               passes evaluate K_s(v) and the test with the same machine
+//               code; separately compiled, the per-voxel parameters' plain
+//               FP32 expressions may be contracted differently and a pair
+//               at its threshold may flip between the passes)
 //   list mode   the CTA's voxels are x.list[bx*(threads*VY) + v*threads + tid]
 //               instead of an image tile (dose / adjoint of listed voxels)
 template <int kMode, int TY, int VY, bool kList = false>
@@ -331,7 +337,7 @@ __device__ __forceinline__ void pb_tile(const Grid &g, const Frame &f, const Pro
                 gv[v] = inside[v] ? __ldg(x.grad_dose + vidx[v]) : 0.0f;
         }
         fill_off[v] = fill_end[v] = 0;
-        if (kMode == kPbFill && inside[v]) {
+        if (kMode == kPbCount && x.row_ptr != nullptr && inside[v]) {
             fill_off[v] = x.row_ptr[vidx[v]];
             fill_end[v] = min(x.row_ptr[vidx[v] + 1], x.cap);  // never past the counted row or the buffers
         }
@@ -498,7 +504,7 @@ __device__ __forceinline__ void pb_tile(const Grid &g, const Frame &f, const Pro
                 float4 a = a2[u], b = b2[u];
                 const int orig = __float_as_int(a.w);
                 if (x.mu) a.z = __ldg(x.mu + orig);
-                if (kMode == kPbCount || kMode == kPbFill) b.w = __ldg(x.thr + orig);
+                if (kMode == kPbCount) b.w = __ldg(x.thr + orig);
                 s_spot_a[pos] = a;
                 s_spot_b[pos] = b;
                 if (kMode == kPbAdjoint) s_acc[pos] = 0.0f;
@@ -616,11 +622,11 @@ __device__ __forceinline__ void pb_tile(const Grid &g, const Frame &f, const Pro
                         if (lane == 0 && m > 0.0f) atomicMax(x.spot_max + __float_as_int(a.w), __float_as_uint(m));
                     } else if (kMode == kPbCount) {
 #pragma unroll
-                        for (int v = 0; v < VY; ++v) cnt[v] += (act[v] && kv[v] >= b.w && kv[v] > 0.0f) ? 1 : 0;
-                    } else if (kMode == kPbFill) {
-#pragma unroll
                         for (int v = 0; v < VY; ++v) {
-                            if (act[v] && kv[v] >= b.w && kv[v] > 0.0f && fill_off[v] < fill_end[v]) {
+                            const bool take = act[v] && kv[v] >= b.w && kv[v] > 0.0f;
+                            if (x.row_ptr == nullptr) {
+                                cnt[v] += take ? 1 : 0;
+                            } else if (take && fill_off[v] < fill_end[v]) {
                                 x.col[fill_off[v]] = __float_as_int(a.w);
                                 x.val[fill_off[v]] = kv[v];
                                 ++fill_off[v];
@@ -639,7 +645,7 @@ __device__ __forceinline__ void pb_tile(const Grid &g, const Frame &f, const Pro
         }
     }
 
-    if (kMode == kPbCount) {
+    if (kMode == kPbCount && x.row_ptr == nullptr) {
 #pragma unroll
         for (int v = 0; v < VY; ++v)
             if (inside[v] && DC_IN_BOUNDS(vidx[v], g.n(), 24)) x.counts[vidx[v]] = cnt[v];
@@ -776,7 +782,10 @@ void launch_pencil_beam_mode(DeviceContext &ctx, int mode, const Grid &g, const 
         case kPbAdjoint: pb_launch<kPbAdjoint>(ctx, "pencil_beam_adjoint", g, f, t, wet_s, nullptr, x, s); break;
         case kPbSpotMax: pb_launch<kPbSpotMax>(ctx, "pencil_beam_spotmax", g, f, t, wet_s, nullptr, x, s); break;
         case kPbCount: pb_launch<kPbCount>(ctx, "pencil_beam_count", g, f, t, wet_s, nullptr, x, s); break;
-        case kPbFill: pb_launch<kPbFill>(ctx, "pencil_beam_fill", g, f, t, wet_s, nullptr, x, s); break;
+        case kPbFill:
+            if (x.row_ptr == nullptr) throw Error(DC_ERR_VALUE, "the fill pass needs the row starts");
+            pb_launch<kPbCount>(ctx, "pencil_beam_fill", g, f, t, wet_s, nullptr, x, s);
+            break;
         default: throw Error(DC_ERR_VALUE, "unknown pencil-beam mode");
     }
 }

@@ -196,6 +196,9 @@ DeviceContext::DeviceContext(int dev) : device(dev) {
     }
     DC_CUDA(cudaSetDevice(dev));
     DC_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    DC_CUDA(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking));
+    DC_CUDA(cudaEventCreateWithFlags(&fork_ev, cudaEventDisableTiming));
+    DC_CUDA(cudaEventCreateWithFlags(&join_ev, cudaEventDisableTiming));
     for (auto &e : pin_ev) DC_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     for (auto &e : stage_ev) DC_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     DC_CUDA(cudaEventCreateWithFlags(&last_use, cudaEventDisableTiming));
@@ -208,6 +211,7 @@ bool DeviceContext::capturing(cudaStream_t s) {
 }
 
 void DeviceContext::begin_call(cudaStream_t s) {
+    head_forked = false;  // a fork left by a call that failed midway is never joined
     if (!capturing(s)) DC_CUDA(cudaStreamWaitEvent(s, last_use, 0));
 }
 
@@ -220,6 +224,8 @@ DeviceContext::~DeviceContext() { release_all(); }
 void DeviceContext::release_all() {
     cudaSetDevice(device);
     if (stream) cudaStreamSynchronize(stream);
+    if (side) cudaStreamSynchronize(side);
+    head_forked = false;
     wet_raw.release();
     vol_a.release();
     vol_b.release();
@@ -228,6 +234,7 @@ void DeviceContext::release_all() {
     active.release();
     xlat.release();
     xstat.release();
+    head.release();
     small.release();
     lut.release();
     tables.release();
@@ -252,6 +259,12 @@ void DeviceContext::release_all() {
     }
     if (last_use) cudaEventDestroy(last_use);
     last_use = nullptr;
+    for (cudaEvent_t *e : {&fork_ev, &join_ev}) {
+        if (*e) cudaEventDestroy(*e);
+        *e = nullptr;
+    }
+    if (side) cudaStreamDestroy(side);
+    side = nullptr;
     if (stream) cudaStreamDestroy(stream);
     stream = nullptr;
 }

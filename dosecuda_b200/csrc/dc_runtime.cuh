@@ -109,6 +109,11 @@ class DeviceContext {
     int device;
     std::mutex mu;
     cudaStream_t stream = nullptr;  // for the host (synchronous) entry points
+    // Side stream for work that runs beside a call's own stream: forked after
+    // fork_ev (recorded on the call's stream), joined through join_ev.
+    cudaStream_t side = nullptr;
+    cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
+    bool head_forked = false;  // photon head factors enqueued on `side`, not yet joined
 
     DeviceBuffer wet_raw;     // unsmoothed WET (cm)
     DeviceBuffer vol_a;       // generic volume scratch (input staging)
@@ -121,6 +126,7 @@ class DeviceContext {
     DeviceBuffer tables;      // proton layer + spot tables
     DeviceBuffer xlat;        // photon ray-lattice integrals G[node][ray] (dc_xray.cu)
     DeviceBuffer xstat;       // voxels the last photon depth pass marched exactly
+    DeviceBuffer head;        // photon head factors (tp, ts, oaf, soft) per voxel, float4
     VolumeArray density;      // density / RLSP texture
     VolumeArray terma;        // TERMA texture (surface-writable)
     // Photon radiological depth: 0 = the reference's per-voxel 1 mm march,

@@ -465,6 +465,27 @@ class ProtonBatch:
         _lib.raise_for(_lib.load().dc_proton_batch_dose(self._h, mp, int(v), C.c_void_p(s.cuda_stream)))
         return self.doses
 
+    def influence_csr(self, beam_id: int, cutoff: float = 1e-4, stream=None):
+        """(row_ptr int64[n_voxels+1], col int32[nnz], val float32[nnz]) of
+        beam ``beam_id``'s voxels x spots influence matrix on its plan's grid
+        (after ``wet()``): entries >= cutoff x the spot's maximum, columns in
+        the beam's spot-list order.  Count, then fill: the only allocations
+        are the returned arrays."""
+        s = stream if stream is not None else torch.cuda.current_stream(self.device)
+        lib = _lib.load()
+        n_vox = self.rlsp[self.beam_plan[beam_id]].numel()
+        row_ptr = torch.empty(n_vox + 1, dtype=torch.int64, device=self.device)
+        nnz = C.c_longlong(0)
+        _lib.raise_for(lib.dc_proton_batch_influence_count(self._h, int(beam_id), float(cutoff),
+                                                            C.c_void_p(row_ptr.data_ptr()), C.byref(nnz),
+                                                            C.c_void_p(s.cuda_stream)))
+        col = torch.empty(max(nnz.value, 1), dtype=torch.int32, device=self.device)
+        val = torch.empty(max(nnz.value, 1), dtype=torch.float32, device=self.device)
+        _lib.raise_for(lib.dc_proton_batch_influence_fill(self._h, int(beam_id), C.c_void_p(row_ptr.data_ptr()),
+                                                           C.c_void_p(col.data_ptr()), C.c_void_p(val.data_ptr()),
+                                                           col.numel(), C.c_void_p(s.cuda_stream)))
+        return row_ptr, col[:nnz.value], val[:nnz.value]
+
     def autotune(self, cache_path: str | None = None, repeats: int = 3) -> int:
         """Time every tile shape of the batch dose kernel on this workload and
         keep the fastest; results are cached in ``cache_path`` (JSON)."""

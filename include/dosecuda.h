@@ -347,6 +347,19 @@ int dc_proton_batch_wet(dc_proton_batch *batch, void *stream);
  * list's order), or NULL to reuse the previous weights (initially the MU
  * column of the spot lists). */
 int dc_proton_batch_dose(dc_proton_batch *batch, const float *mu_dev, int variant, void *stream);
+/* Influence matrix of one beam (beam_id in add order; after
+ * dc_proton_batch_wet), count-then-fill, one beam at a time so that memory
+ * stays bounded by the largest beam's matrix.  Voxel rows of the beam's plan
+ * grid, spot columns in the beam's spot-list order, entries K_s(v) >= cutoff
+ * * max_v K_s(v) (the entries dc_proton_beam_influence_csr gives for the
+ * same beam and WET).  _count writes the row starts (n_voxels + 1 int64)
+ * into row_ptr_dev and the entry count into *nnz (synchronises); _fill
+ * then writes col_dev (int32) and val_dev (float32, dose per MU) for the
+ * beam _count ran last, capacity >= nnz.  No counterpart in the reference. */
+int dc_proton_batch_influence_count(dc_proton_batch *batch, int beam_id, float cutoff, long long *row_ptr_dev,
+                                    long long *nnz, void *stream);
+int dc_proton_batch_influence_fill(dc_proton_batch *batch, int beam_id, const long long *row_ptr_dev, int *col_dev,
+                                   float *val_dev, long long capacity, void *stream);
 int dc_proton_batch_destroy(dc_proton_batch *batch);
 
 /* ------------------------------------------------------------------ */

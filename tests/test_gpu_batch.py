@@ -62,6 +62,42 @@ def test_batch_anisotropic_plan_matches_oracle(batch):
     assert dose_diff(b.doses[pid].cpu().numpy(), ref) <= 1e-3
 
 
+def test_batch_influence_matrix_equals_the_per_beam_matrix(batch):
+    """Count-then-fill CSR of every beam of the batch against the single-beam
+    entry point on the same WET (the same kernels: equal arrays), and the
+    matrix-vector product of the plan's beams against the batch dose."""
+    torch, engine, model, b, plans = batch
+    for grid, beams, rl, pid, ids in plans[:2]:
+        total = torch.zeros(rl.numel(), dtype=torch.float64, device="cuda")
+        for bm, bid in zip(beams, ids):
+            r, c, v = b.influence_csr(bid, cutoff=1e-4)
+            r0, c0, v0 = engine.ProtonBeamPlan(grid, bm, model).influence_csr(b.wets[bid], cutoff=1e-4)
+            torch.cuda.synchronize()
+            assert int(r[-1]) == c.numel() > 0
+            # the single-beam call zero-fills its arrays before the fill pass,
+            # so an entry counted but never filled would show as a zero
+            assert bool((v0 > 0).all())
+            assert torch.equal(r, r0) and torch.equal(c, c0) and torch.equal(v, v0)
+            a = torch.sparse_csr_tensor(r, c.long(), v.double(), size=(rl.numel(), bm.spot_list.shape[0]))
+            mu = torch.as_tensor(np.asarray(bm.spot_list, np.float64)[:, 2], device="cuda")
+            total += (a @ mu.unsqueeze(1)).squeeze(1)
+        b.dose(b.mu0)
+        torch.cuda.synchronize()
+        d = b.doses[pid].reshape(-1).double()
+        # entries below 1e-4 of their spot's maximum are dropped from the matrix
+        assert float((total - d).abs().max()) <= 2e-3 * float(d.max())
+    # host-side checks, before any launch: NULL buffers, and a fill for a beam
+    # other than the one counted last
+    lib = engine._lib.load()
+    first = plans[0][4][0]
+    with pytest.raises(ValueError):
+        engine._lib.raise_for(lib.dc_proton_batch_influence_fill(b._h, first, None, None, None, 0, None))
+    buf = torch.zeros(16, dtype=torch.int64, device="cuda")
+    with pytest.raises(ValueError):
+        engine._lib.raise_for(lib.dc_proton_batch_influence_fill(b._h, first, buf.data_ptr(), buf.data_ptr(),
+                                                                 buf.data_ptr(), 16, None))
+
+
 def test_tile_variants_agree_and_autotune(batch, tmp_path):
     torch, engine, model, b, plans = batch
     base = [d.clone() for d in b.dose(variant=0)]
