@@ -266,6 +266,34 @@ def run_mine(args, ws, rank, local, dist_mod):
     depth_mode = engine.photon_depth_mode(local)
     depth_marched = engine.photon_depth_marched(local)
     dose_np = dose_t.cpu().numpy()
+
+    # the cone-direction sweep CCCS (an approximation, not the headline) beside
+    # the per-voxel CCCS of the same TERMA: time and distance from it
+    xbeam = engine.PhotonBeam(grid, dens_t.shape, device=dev)
+    xbeam.set_density(dens_t)
+    xbeam.terma(model, cp, views=views)
+    exact, sweep = xbeam.dose(), xbeam.dose_sweep()
+    torch.cuda.synchronize()
+    sev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    sev[0].record()
+    for _ in range(args.steps):
+        xbeam.dose(out=exact)
+    sev[1].record()
+    sev[2].record()
+    for _ in range(args.steps):
+        xbeam.dose_sweep(out=sweep)
+    sev[3].record()
+    torch.cuda.synchronize()
+    gc = engine.gamma_counts(sweep, grid.spacing, exact).cpu().numpy()
+    e_np, s_np = exact.cpu().numpy().astype(np.float64), sweep.cpu().numpy().astype(np.float64)
+    hi = e_np > 0.1 * e_np.max()
+    sweep_rec = {"ms_sweep": round(sev[2].elapsed_time(sev[3]) / args.steps, 4),
+                 "ms_per_voxel_cccs": round(sev[0].elapsed_time(sev[1]) / args.steps, 4),
+                 "dD_frac_dmax": round(float(np.abs(s_np - e_np)[hi].max() / e_np.max()), 5),
+                 "gamma_2_2": round(float(gc[1]) / max(int(gc[0]), 1), 5),
+                 "what": "dc_photon_beam_dose_sweep against dc_photon_beam_dose on the same TERMA (CCCS only, "
+                         "no ray trace or TERMA); an approximation outside the parity bar, not the headline"}
+    xbeam.close()
     # active voxels = TERMA > 0.01 (the voxels the CCCS evaluates); from the
     # engine's TERMA mask we only need the count, taken as dose > 0 voxels.
     n_active = int((dose_np > 0).sum())
@@ -284,6 +312,10 @@ def run_mine(args, ws, rank, local, dist_mod):
     # call: the headline passes the pageable array DensityFromHU returns, as
     # the reference's plan loop does (plan_imrt.py:126-158); the same call
     # with a page-locked input is reported beside it
+    # calls per end-to-end leg: the K steps, and at least 30 so that the
+    # wall-clock mean spans tens of milliseconds
+    n_e2e = max(args.steps, 30)
+
     def e2e_photon(voxels):
         vol = VolumeObject()
         vol.voxel_data = voxels
@@ -294,17 +326,13 @@ def run_mine(args, ws, rank, local, dist_mod):
         torch.cuda.synchronize()
         barrier(dist_mod)
         t0 = time.perf_counter()
-        for _ in range(args.steps):
+        for _ in range(n_e2e):
             d = dose_kernels.photon_dose_cuda(model, vol, cp, local)
         torch.cuda.synchronize()
         ms = (time.perf_counter() - t0) * 1e3
         barrier(dist_mod)
         return aggregate_max(ms, dist_mod), d
 
-    e2e_ms, d = e2e_photon(density)
-    pinned = torch.from_numpy(density).pin_memory()
-    e2e_pinned_ms, _ = e2e_photon(pinned.numpy())
-    parity_e2e = float(np.abs(d - dose_np).max())
 
     # ---------------- proton (secondary) ----------------
     pgrid, pmodel, pbeam, rlsp = proton_workload()
@@ -324,7 +352,15 @@ def run_mine(args, ws, rank, local, dist_mod):
     torch.cuda.synchronize()
     barrier(dist_mod)
     tp_ms = time_steps(step_p, args.steps, flush)
-    clk.__exit__(None, None, None)
+    clk.__exit__(None, None, None)  # the device-timed regions end here
+
+    # end-to-end legs after the clock sampler has stopped: its polling takes
+    # driver locks that stall host API calls, which a wall-clock figure over a
+    # few milliseconds would pick up
+    e2e_ms, d = e2e_photon(density)
+    pinned = torch.from_numpy(density).pin_memory()
+    e2e_pinned_ms, _ = e2e_photon(pinned.numpy())
+    parity_e2e = float(np.abs(d - dose_np).max())
     barrier(dist_mod)
     tp_ms = aggregate_max(tp_ms, dist_mod)
     spots_per_s = n_spots * args.steps * ws / (tp_ms * 1e-3)
@@ -362,7 +398,7 @@ def run_mine(args, ws, rank, local, dist_mod):
             beam_call()
         barrier(dist_mod)
         t0 = time.perf_counter()
-        for _ in range(args.steps):
+        for _ in range(n_e2e):
             beam_call()
         ms = (time.perf_counter() - t0) * 1e3
         barrier(dist_mod)
@@ -376,7 +412,8 @@ def run_mine(args, ws, rank, local, dist_mod):
         n_active=n_active, cccs_avg_ms=cccs_avg_ms, achieved_tf=achieved_tf, fp32_peak=fp32_peak,
         cccs_bytes=cccs_bytes, e2e_ms=e2e_ms, e2e_pinned_ms=e2e_pinned_ms, parity_e2e=parity_e2e, nvox=nvox, pk=pk,
         pk_kind=pk_kind, spots_per_s=spots_per_s, tp_ms=tp_ms, prof_p=prof_p, pairs=pairs, pb_avg_ms=pb_avg_ms,
-        pe2e_ms=pe2e_ms, pe2e_pinned_ms=pe2e_pinned_ms, n_spots=n_spots, pnvox=rlsp.size,
+        pe2e_ms=pe2e_ms, pe2e_pinned_ms=pe2e_pinned_ms, n_spots=n_spots, pnvox=rlsp.size, n_e2e=n_e2e,
+        sweep=sweep_rec,
     ))
     return out
 
@@ -900,12 +937,12 @@ def main_mine(args):
                        "step": "one control point: ray trace + TERMA + CCCS, density resident in HBM",
                        "l2": "flushed between steps (256 MiB write, outside the timed brackets)",
                        "parallelism": "replicas" if ws > 1 else "single GPU"},
-            "e2e": {"value": round(r["e2e_ms"] / (args.steps * ws), 4), "unit": "ms/beam",
+            "e2e": {"value": round(r["e2e_ms"] / (r["n_e2e"] * ws), 4), "unit": "ms/beam", "calls": r["n_e2e"],
                     "h2d_bytes_per_step": int(r["nvox"] * 4), "d2h_bytes_per_step": int(r["nvox"] * 4),
                     "api": "dosecuda_b200.dose_kernels.photon_dose_cuda (host numpy in/out: the pageable density "
                            "array DensityFromHU returns, as the reference's plan loop passes it; the returned "
                            "array page-locked by the call)",
-                    "pinned_input": {"value": round(r["e2e_pinned_ms"] / (args.steps * ws), 4), "unit": "ms/beam",
+                    "pinned_input": {"value": round(r["e2e_pinned_ms"] / (r["n_e2e"] * ws), 4), "unit": "ms/beam",
                                      "what": "the same call with a page-locked input array"}},
             # The CCCS's binding unit is the texture pipe (one filtered float2
             # fetch per cone sample; L1TEX ~95 % busy under ncu), so the
@@ -938,6 +975,7 @@ def main_mine(args):
             "kernels": {k: {"launches": v[0], "total_ms": round(v[1], 4)} for k, v in r["prof_x"].items()},
             "stages": stage_rates(r["prof_x"], r["nvox"], march_x, fetch_rate),
             "depth_pass": depth_stage(r),
+            "cccs_sweep": r["sweep"],
             "gpu_launches": x_launch_per_step * args.steps,
             "clocks": r["clocks"],
             "cpu_baseline": cpu_x,
@@ -950,12 +988,13 @@ def main_mine(args):
                 "config": {"workload": "proton PB small: 96^3 @ 2 mm, water + bone cylinder + lung slab, gantry 0, "
                                        "6 layers (energy ids 34..59) x 100 spots",
                            "step": "one beam: WET ray trace + smoothing + pencil-beam dose, RLSP resident in HBM"},
-                "e2e": {"value": round(r["n_spots"] * args.steps * ws / (r["pe2e_ms"] * 1e-3), 1), "unit": "spots/s",
+                "e2e": {"value": round(r["n_spots"] * r["n_e2e"] * ws / (r["pe2e_ms"] * 1e-3), 1), "unit": "spots/s",
+                        "calls": r["n_e2e"],
                         "h2d_bytes_per_step": int(r["pnvox"] * 4 * 2), "d2h_bytes_per_step": int(r["pnvox"] * 4 * 2),
                         "api": "dose_kernels.proton_raytrace_cuda + proton_spot_cuda (host numpy: the pageable "
                                "RLSP array RLSPFromHU returns, the WET passed back as a fresh array copy, as "
                                "the reference's plan loop does)",
-                        "pinned_input": {"value": round(r["n_spots"] * args.steps * ws / (r["pe2e_pinned_ms"] * 1e-3),
+                        "pinned_input": {"value": round(r["n_spots"] * r["n_e2e"] * ws / (r["pe2e_pinned_ms"] * 1e-3),
                                                         1), "unit": "spots/s",
                                          "what": "the same calls with a page-locked RLSP array"}},
                 "roofline": pencil_beam_roofline(r),
@@ -1012,11 +1051,12 @@ def main_reference(args):
     vol.spacing = np.array(grid.spacing, dtype=np.single)
     for _ in range(args.warmup):
         ref.photon_dose_cuda(model, vol, cp, local)
+    n_calls = max(args.steps, 30)  # as the end-to-end legs of this engine's arm
     with ClockSampler(local) as clk:
         t0 = time.perf_counter()
-        for _ in range(args.steps):
+        for _ in range(n_calls):
             ref.photon_dose_cuda(model, vol, cp, local)
-        x_ms = (time.perf_counter() - t0) * 1e3 / args.steps
+        x_ms = (time.perf_counter() - t0) * 1e3 / n_calls
 
     pgrid, pmodel, pbeam, rlsp = proton_workload()
     pvol = VolumeObject()
@@ -1025,17 +1065,19 @@ def main_reference(args):
     pvol.spacing = np.array(pgrid.spacing, dtype=np.single)
 
     def beam_step():
+        # the reference's plan loop (plan_impt.py:124-160): WET, then the dose
+        # from a fresh array copy of it, as this engine's end-to-end leg does
         w = ref.proton_raytrace_cuda(pmodel, pvol, pbeam, local)
         wv = VolumeObject()
-        wv.voxel_data, wv.origin, wv.spacing = w, pvol.origin, pvol.spacing
+        wv.voxel_data, wv.origin, wv.spacing = np.array(w, dtype=np.single), pvol.origin, pvol.spacing
         ref.proton_spot_cuda(pmodel, pvol, wv, pbeam, local)
 
     for _ in range(args.warmup):
         beam_step()
     t0 = time.perf_counter()
-    for _ in range(args.steps):
+    for _ in range(n_calls):
         beam_step()
-    p_s = (time.perf_counter() - t0) / args.steps
+    p_s = (time.perf_counter() - t0) / n_calls
     n_spots = pbeam.spot_list.shape[0]
 
     batched = None
@@ -1088,7 +1130,8 @@ def main_reference(args):
                                "10x10 cm MLC field, 100 MU, gantry 0, 72 cone directions",
                    "step": "one control point through the reference's dose_kernels.photon_dose_cuda",
                    "parallelism": "single GPU"},
-        "e2e": {"value": round(x_ms, 4), "unit": "ms/beam", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "e2e": {"value": round(x_ms, 4), "unit": "ms/beam", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0,
+                "calls": n_calls},
         "cpu_baseline": {"value": round(x_ms, 4), "unit": "ms/beam", "cores": 1, "kind": "reference",
                          "sample": "the reference's own implementation is CUDA-only: its extension (%s) built from "
                                    "the reference sources for sm_100a, run on the B200 through its Python API with "
@@ -1097,7 +1140,7 @@ def main_reference(args):
         "clocks": clk.summary(),
         "secondary": {"metric": "IMPT spots/s", "value": round(n_spots / p_s, 1), "unit": "spots/s",
                       "higher_is_better": True, "ms_per_step": round(p_s * 1e3, 4),
-                      "e2e": {"value": round(n_spots / p_s, 1), "unit": "spots/s"}},
+                      "e2e": {"value": round(n_spots / p_s, 1), "unit": "spots/s", "calls": n_calls}},
         "batched": batched,
         "plan_loop": plan_loop,
     }

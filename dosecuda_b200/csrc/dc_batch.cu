@@ -273,12 +273,9 @@ int dc_proton_batch_commit(dc_proton_batch *b) {
                          [&](int x, int y) { return b->plans[x].cost > b->plans[y].cost; });
         const int nv = pencil_beam_batch_variants();
         for (int v = 0; v < nv && v < 8; ++v) {
-            int ty = 0, vy = 0;
-            pencil_beam_batch_tile(v, &ty, &vy);
             std::vector<int2> items;
             for (int pi : plan_order) {
-                const Grid &g = b->plans[pi].g;
-                const long long tiles = (long long)((g.nx + 31) / 32) * ((g.ny + ty * vy - 1) / (ty * vy)) * g.nz;
+                const long long tiles = pencil_beam_batch_tiles(v, b->plans[pi].g);
                 need(tiles < 0x7fffffffLL, "plan too large for the batch work queue.");
                 for (long long t = 0; t < tiles; ++t) items.push_back(make_int2(pi, (int)t));
             }

@@ -152,10 +152,11 @@ struct PbBatchPlan {
     int beam0, n_beams;
 };
 
-// Work items are (plan, tile) pairs; tile = k * tiles_x * tiles_y + by * tiles_x + bx
+// Work items are (plan, tile) pairs; tile = bz * tiles_x * tiles_y + by * tiles_x + bx
 // for the variant's tile shape.  `next` is the device queue head (reset here).
 int pencil_beam_batch_variants();
-void pencil_beam_batch_tile(int variant, int *threads_y, int *voxels_y);
+void pencil_beam_batch_tile(int variant, int *threads_y, int *voxels_per_thread);
+long long pencil_beam_batch_tiles(int variant, const Grid &g);  // tiles of grid g
 void launch_pencil_beam_batch(DeviceContext &ctx, int variant, const PbBatchPlan *plans, const PbBatchBeam *beams,
                               const int2 *items, int n_items, unsigned *next, int lut_len, cudaStream_t s);
 

@@ -15,8 +15,8 @@
 // spot's divergent axis.
 //
 // B200 mapping (instead of one thread per (voxel, layer) with a global
-// atomicAdd per pair of the reference): a CTA owns a 32x16 tile of voxels in
-// one z-slice, two voxels per thread, and walks all energy layers.  Per layer
+// atomicAdd per pair of the reference): a CTA owns a 16x8x4 tile of voxels,
+// two voxels per thread, and walks all energy layers.  Per layer
 // the CTA stages the layer's LUT rows and spot records in shared memory
 // (broadcast reads in the spot loop); each thread keeps its voxels' dose in
 // registers across layers and writes each voxel once — no atomics, so the
@@ -42,8 +42,38 @@ DC_BOUNDS_WORD
 
 constexpr int kPbThreadsX = 32;
 constexpr int kPbThreadsY = 8;
-constexpr int kPbVoxY = 2;      // voxels per thread along y
+constexpr int kPbVoxY = 2;      // voxels per thread
 constexpr int kPbSpotChunk = 512;
+// Voxel tile of one CTA: the 32 lanes of a warp split kPbLanesX along x and
+// kPbLanesZ along z, the warps (threadIdx.y) lie along y, and a thread's VY
+// voxels step along z, so a tile is kPbLanesX x TY x (kPbLanesZ * VY) voxels
+// (16 x 8 x 4 for the default shape).  A tile compact in all three axes has
+// a smaller beam's-eye-view footprint whatever the beam direction, which
+// keeps the per-CTA lateral cut-off tighter: a flat 32 x 16 x 1 tile reaches
+// 64 mm across at 2 mm voxels and evaluates every spot within the cut-off of
+// any of its voxels for all 512 of them.  Measured (96^3 beam; 4 plans of the
+// batched workload): 32x16x1 0.195-0.205 ms / 18.0 ms, 8x8x8 0.181-0.186 /
+// 17.0, 16x8x4 0.184 / 16.7, 4x8x16 0.188 / 19.1.
+constexpr int kPbLanesX = 16;
+constexpr int kPbLanesZ = kPbThreadsX / kPbLanesX;
+static_assert(kPbLanesX * kPbLanesZ == kPbThreadsX, "lanes of a warp tile x and z");
+template <int TY, int VY>
+struct PbTileShape {
+    static constexpr int x = kPbLanesX, y = TY, z = kPbLanesZ * VY;
+};
+// Tiles of a grid along each axis for the shape, and the voxel (i, j, k) of
+// this thread's voxel v in tile (bx, by, bz) (possibly outside the grid).
+template <int TY, int VY>
+__host__ __device__ __forceinline__ int3 pb_tiles(const Grid &g) {
+    using S = PbTileShape<TY, VY>;
+    return make_int3((g.nx + S::x - 1) / S::x, (g.ny + S::y - 1) / S::y, (g.nz + S::z - 1) / S::z);
+}
+template <int TY, int VY>
+__device__ __forceinline__ int3 pb_tile_voxel(int bx, int by, int bz, int v) {
+    using S = PbTileShape<TY, VY>;
+    return make_int3(bx * S::x + (int)(threadIdx.x % kPbLanesX), by * S::y + (int)threadIdx.y,
+                     bz * S::z + (int)(threadIdx.x / kPbLanesX) + kPbLanesZ * v);
+}
 static_assert(2 * kPbThreadsX * kPbThreadsY == kPbSpotChunk, "two spots per thread per staging round");
 
 void build_proton_tables(const float *spots, int n_spots, const float *dvp, int n_energies, int dvp_len,
@@ -151,21 +181,36 @@ __device__ __forceinline__ bool pb_voxel_layer(const LayerRec &L, const float *s
     return true;
 }
 
-// Squared distance from two voxels (packed lanes) to one spot's divergent
-// axis, on the paired-lane FP32 instructions of sm_100 (fma.rn.f32x2 and
-// friends: one issue for both voxels).  Each lane performs exactly the
-// scalar sequence
-//   rx = hx - sx,  ry = hy - sy,  ray2 = fma(rx, rx, fma(ry, ry, hz^2)),
-//   dot = fma(tx, rx, fma(ty, ry, -hz)),  r2 = fma(-dot, dot * inv_t2, ray2)
-// (the negations are moved onto exactly negated operands), so the packed and
-// the scalar forms agree bit for bit.
-__device__ __forceinline__ float2 pb_r2_pair(float2 hx, float2 hy, float2 hz2, float2 nhz, float2 nsx, float2 nsy,
-                                            float2 tx, float2 ty, float2 ninv_t2) {
+// Squared distance from a voxel to one spot's divergent axis (caxDistance,
+// IMPTClasses.cu:123-133), r^2 = |ray|^2 - (t.ray)^2 / |t|^2 with
+// ray = (hx - sx, hy - sy, hz) and t = (tx, ty, -1), evaluated as
+// |ray x t|^2 / |t|^2 (the same quantity by Lagrange's identity).  The
+// reference's form subtracts two squares of ~|hz|^2 (4e4 mm^2 at 200 mm from
+// the isocentre), so its float rounding moves r^2 by ~0.01 mm^2 and a far
+// pair's Gaussian by ~1e-4; the cross product has no such cancellation and
+// holds the FP64 value to a few ulps of r^2 itself.  With t_z = -1:
+//   ray x t = (-(ry + hz ty), rx + hz tx, rx ty - ry tx).
+__device__ __forceinline__ float pb_r2(float hx, float hy, float hz, float sx, float sy, float tx, float ty,
+                                       float inv_t2) {
+    const float rx = __fsub_rn(hx, sx), ry = __fsub_rn(hy, sy);
+    const float cu = __fmaf_rn(hz, tx, rx), cw = __fmaf_rn(hz, ty, ry);
+    const float cc = __fmaf_rn(rx, ty, __fmul_rn(ry, -tx));
+    return __fmul_rn(__fmaf_rn(cu, cu, __fmaf_rn(cw, cw, __fmul_rn(cc, cc))), inv_t2);
+}
+
+// The same for two voxels (packed lanes) on the paired-lane FP32
+// instructions of sm_100 (fma.rn.f32x2 and friends: one issue for both
+// voxels).  Each lane performs exactly pb_r2's sequence (the negations are
+// moved onto exactly negated operands: nsx = -sx, nsy = -sy, ntx = -tx), so
+// the packed and the scalar forms agree bit for bit.
+__device__ __forceinline__ float2 pb_r2_pair(float2 hx, float2 hy, float2 hz, float2 nsx, float2 nsy, float2 tx,
+                                            float2 ty, float2 ntx, float2 inv_t2) {
     const float2 rx = __fadd2_rn(hx, nsx);
     const float2 ry = __fadd2_rn(hy, nsy);
-    const float2 ray2 = __ffma2_rn(rx, rx, __ffma2_rn(ry, ry, hz2));
-    const float2 dot = __ffma2_rn(tx, rx, __ffma2_rn(ty, ry, nhz));
-    return __ffma2_rn(dot, __fmul2_rn(dot, ninv_t2), ray2);
+    const float2 cu = __ffma2_rn(hz, tx, rx);
+    const float2 cw = __ffma2_rn(hz, ty, ry);
+    const float2 cc = __ffma2_rn(rx, ty, __fmul2_rn(ry, ntx));
+    return __fmul2_rn(__ffma2_rn(cu, cu, __ffma2_rn(cw, cw, __fmul2_rn(cc, cc))), inv_t2);
 }
 
 __device__ __forceinline__ float2 f2(float v) { return make_float2(v, v); }
@@ -271,7 +316,7 @@ void launch_layer_rcut(const Grid &g, const Frame &f, LayerRec *layers, int n_la
 //               instead of an image tile (dose / adjoint of listed voxels)
 template <int kMode, int TY, int VY, bool kList = false>
 __device__ __forceinline__ void pb_tile(const Grid &g, const Frame &f, const ProtonTables &t,
-                                        const float *__restrict__ wet_s, int bx, int by, int k, float (&acc)[VY],
+                                        const float *__restrict__ wet_s, int bx, int by, int bz, float (&acc)[VY],
                                         const PbExtra &x) {
     extern __shared__ float4 smem4[];
     float4 *s_spot_a = smem4;                    // x, y, mu, orig (int bits)
@@ -288,11 +333,9 @@ __device__ __forceinline__ void pb_tile(const Grid &g, const Frame &f, const Pro
     const int tid = threadIdx.y * kPbThreadsX + threadIdx.x;
     const int lane = threadIdx.x;
     const int nthreads = kThreads;
-    const int i = bx * kPbThreadsX + threadIdx.x;
-    const int j0 = by * (TY * VY) + threadIdx.y;
     __syncthreads();  // shared memory of a previous tile (persistent caller) no longer in use
 
-    float hx[VY], hy[VY], hz[VY], hz2[VY], wet_mm[VY], dsrc[VY];
+    float hx[VY], hy[VY], hz[VY], wet_mm[VY], dsrc[VY];
     float gv[VY];
     long long vidx[VY];
     long long fill_off[VY], fill_end[VY];
@@ -313,12 +356,12 @@ __device__ __forceinline__ void pb_tile(const Grid &g, const Frame &f, const Pro
             jc = (int)(rem / g.nx);
             ic = (int)(rem - (long long)jc * g.nx);
         } else {
-            const int j = j0 + v * TY;
-            inside[v] = (i < g.nx) && (j < g.ny);
-            ic = min(i, g.nx - 1);
-            jc = min(j, g.ny - 1);
-            kc = k;
-            vidx[v] = (long long)ic + (long long)g.nx * (jc + (long long)g.ny * k);
+            const int3 q = pb_tile_voxel<TY, VY>(bx, by, bz, v);
+            inside[v] = q.x < g.nx && q.y < g.ny && q.z < g.nz;
+            ic = min(q.x, g.nx - 1);
+            jc = min(q.y, g.ny - 1);
+            kc = min(q.z, g.nz - 1);
+            vidx[v] = (long long)ic + (long long)g.nx * (jc + (long long)g.ny * kc);
         }
         cnt[v] = 0;
         const float3 p = voxel_xyz(g, f, ic, jc, kc);
@@ -326,7 +369,6 @@ __device__ __forceinline__ void pb_tile(const Grid &g, const Frame &f, const Pro
         hx[v] = h.x;
         hy[v] = h.y;
         hz[v] = h.z;
-        hz2[v] = h.z * h.z;
         dsrc[v] = distance_to_source(f, p);
         wet_mm[v] = (DC_IN_BOUNDS(vidx[v], g.n(), 21) ? __ldg(wet_s + vidx[v]) : 0.0f) * 10.0f;
         gv[v] = 0.0f;
@@ -516,13 +558,12 @@ __device__ __forceinline__ void pb_tile(const Grid &g, const Frame &f, const Pro
                 if (!any) continue;
                 // voxels (2p, 2p+1) of the thread share the paired lanes of p
                 constexpr int VP = VY / 2;
-                float2 hxp[VP], hyp[VP], hz2p[VP], nhzp[VP], ps2p[VP], hs2p[VP], accp[VP], acch[VP];
+                float2 hxp[VP], hyp[VP], hzp[VP], ps2p[VP], hs2p[VP], accp[VP], acch[VP];
 #pragma unroll
                 for (int p = 0; p < VP; ++p) {
                     hxp[p] = make_float2(hx[2 * p], hx[2 * p + 1]);
                     hyp[p] = make_float2(hy[2 * p], hy[2 * p + 1]);
-                    hz2p[p] = make_float2(hz2[2 * p], hz2[2 * p + 1]);
-                    nhzp[p] = make_float2(-hz[2 * p], -hz[2 * p + 1]);
+                    hzp[p] = make_float2(hz[2 * p], hz[2 * p + 1]);
                     ps2p[p] = make_float2(pv[2 * p].ps2, pv[2 * p + 1].ps2);
                     hs2p[p] = make_float2(pv[2 * p].hs2, pv[2 * p + 1].hs2);
                     accp[p] = acch[p] = f2(0.f);
@@ -531,11 +572,11 @@ __device__ __forceinline__ void pb_tile(const Grid &g, const Frame &f, const Pro
                 for (int q = 0; q < cn; ++q) {
                     const float4 a = s_spot_a[q];
                     const float4 b = s_spot_b[q];
-                    const float2 nsx = f2(-a.x), nsy = f2(-a.y), tx = f2(b.x), ty = f2(b.y), nit = f2(-b.z);
-                    const float2 mu = f2(a.z);
+                    const float2 nsx = f2(-a.x), nsy = f2(-a.y), tx = f2(b.x), ty = f2(b.y), ntx = f2(-b.x);
+                    const float2 it2 = f2(b.z), mu = f2(a.z);
 #pragma unroll
                     for (int p = 0; p < VP; ++p) {
-                        const float2 r2 = pb_r2_pair(hxp[p], hyp[p], hz2p[p], nhzp[p], nsx, nsy, tx, ty, nit);
+                        const float2 r2 = pb_r2_pair(hxp[p], hyp[p], hzp[p], nsx, nsy, tx, ty, ntx, it2);
                         accp[p] = __ffma2_rn(mu, exp2_pair(__fmul2_rn(ps2p[p], r2)), accp[p]);
                         acch[p] = __ffma2_rn(mu, exp2_pair(__fmul2_rn(hs2p[p], r2)), acch[p]);
                     }
@@ -556,11 +597,7 @@ __device__ __forceinline__ void pb_tile(const Grid &g, const Frame &f, const Pro
                     const float4 b = s_spot_b[q];
 #pragma unroll
                     for (int v = 0; v < VY; ++v) {
-                        const float rx = hx[v] - a.x;
-                        const float ry = hy[v] - a.y;
-                        const float ray2 = fmaf(rx, rx, fmaf(ry, ry, hz2[v]));
-                        const float dot = fmaf(b.x, rx, fmaf(b.y, ry, -hz[v]));
-                        const float r2 = fmaf(-dot, dot * b.z, ray2);
+                        const float r2 = pb_r2(hx[v], hy[v], hz[v], a.x, a.y, b.x, b.y, b.z);
                         accp[v] = fmaf(a.z, fast_exp2(pv[v].ps2 * r2), accp[v]);
                         acch[v] = fmaf(a.z, fast_exp2(pv[v].hs2 * r2), acch[v]);
                     }
@@ -579,13 +616,13 @@ __device__ __forceinline__ void pb_tile(const Grid &g, const Frame &f, const Pro
                     const float4 b = s_spot_b[q];
                     float kv[VY];
                     if constexpr (VY % 2 == 0) {
-                        const float2 nsx = f2(-a.x), nsy = f2(-a.y), tx = f2(b.x), ty = f2(b.y), nit = f2(-b.z);
+                        const float2 nsx = f2(-a.x), nsy = f2(-a.y), tx = f2(b.x), ty = f2(b.y), ntx = f2(-b.x);
+                        const float2 it2 = f2(b.z);
 #pragma unroll
                         for (int p = 0; p < VY / 2; ++p) {
                             const int v0 = 2 * p, v1 = 2 * p + 1;
                             const float2 r2 = pb_r2_pair(make_float2(hx[v0], hx[v1]), make_float2(hy[v0], hy[v1]),
-                                                         make_float2(hz2[v0], hz2[v1]), make_float2(-hz[v0], -hz[v1]),
-                                                         nsx, nsy, tx, ty, nit);
+                                                         make_float2(hz[v0], hz[v1]), nsx, nsy, tx, ty, ntx, it2);
                             const float2 ep = exp2_pair(__fmul2_rn(make_float2(pv[v0].ps2, pv[v1].ps2), r2));
                             const float2 eh = exp2_pair(__fmul2_rn(make_float2(pv[v0].hs2, pv[v1].hs2), r2));
                             const float2 k2 = __ffma2_rn(make_float2(pv[v0].pf, pv[v1].pf), ep,
@@ -596,11 +633,7 @@ __device__ __forceinline__ void pb_tile(const Grid &g, const Frame &f, const Pro
                     } else {
 #pragma unroll
                         for (int v = 0; v < VY; ++v) {
-                            const float rx = hx[v] - a.x;
-                            const float ry = hy[v] - a.y;
-                            const float ray2 = fmaf(rx, rx, fmaf(ry, ry, hz2[v]));
-                            const float dot = fmaf(b.x, rx, fmaf(b.y, ry, -hz[v]));
-                            const float r2 = fmaf(-dot, dot * b.z, ray2);
+                            const float r2 = pb_r2(hx[v], hy[v], hz[v], a.x, a.y, b.x, b.y, b.z);
                             kv[v] = act[v] ? fmaf(pv[v].pf, fast_exp2(pv[v].ps2 * r2),
                                                   pv[v].hf * fast_exp2(pv[v].hs2 * r2))
                                            : 0.0f;
@@ -662,7 +695,7 @@ __device__ __forceinline__ void pb_tile(const Grid &g, const Frame &f, const Pro
 // the spot loop.
 constexpr int pb_min_ctas(int ty, int per_256) { return ty >= 8 ? per_256 : 2 * per_256; }
 
-// One tile per CTA (grid = tiles of the volume x slices).
+// One tile per CTA (grid = the tiles of the volume, pb_tiles).
 template <int kMode, int TY, int VY>
 __global__ void __launch_bounds__(kPbThreadsX *TY, pb_min_ctas(TY, 4))
     pb_kernel(Grid g, Frame f, ProtonTables t, const float *__restrict__ wet_s, float *__restrict__ dose, PbExtra x) {
@@ -671,12 +704,11 @@ __global__ void __launch_bounds__(kPbThreadsX *TY, pb_min_ctas(TY, 4))
     for (int v = 0; v < VY; ++v) acc[v] = 0.0f;
     pb_tile<kMode, TY, VY>(g, f, t, wet_s, blockIdx.x, blockIdx.y, blockIdx.z, acc, x);
     if (kMode == kPbDose) {
-        const int i = blockIdx.x * kPbThreadsX + threadIdx.x;
 #pragma unroll
         for (int v = 0; v < VY; ++v) {
-            const int j = blockIdx.y * (TY * VY) + threadIdx.y + v * TY;
-            const long long u = (long long)i + (long long)g.nx * (j + (long long)g.ny * blockIdx.z);
-            if (i < g.nx && j < g.ny && DC_IN_BOUNDS(u, g.n(), 20)) dose[u] = acc[v];
+            const int3 q = pb_tile_voxel<TY, VY>(blockIdx.x, blockIdx.y, blockIdx.z, v);
+            const long long u = (long long)q.x + (long long)g.nx * (q.y + (long long)g.ny * q.z);
+            if (q.x < g.nx && q.y < g.ny && q.z < g.nz && DC_IN_BOUNDS(u, g.n(), 20)) dose[u] = acc[v];
         }
     }
 }
@@ -717,11 +749,10 @@ __global__ void __launch_bounds__(kPbThreadsX *TY, pb_min_ctas(TY, 3))
         if (it >= n_items) break;
         const int2 w = items[it];
         const PbBatchPlan P = plans[w.x];
-        const int tiles_x = (P.g.nx + kPbThreadsX - 1) / kPbThreadsX;
-        const int tiles_y = (P.g.ny + TY * VY - 1) / (TY * VY);
-        const int k = w.y / (tiles_x * tiles_y);
-        const int rem = w.y - k * tiles_x * tiles_y;
-        const int by = rem / tiles_x, bx = rem - by * tiles_x;
+        const int3 nt = pb_tiles<TY, VY>(P.g);
+        const int bz = w.y / (nt.x * nt.y);
+        const int rem = w.y - bz * nt.x * nt.y;
+        const int by = rem / nt.x, bx = rem - by * nt.x;
         float acc[VY];
 #pragma unroll
         for (int v = 0; v < VY; ++v) acc[v] = 0.0f;
@@ -729,14 +760,13 @@ __global__ void __launch_bounds__(kPbThreadsX *TY, pb_min_ctas(TY, 3))
             const PbBatchBeam B = beams[b];
             PbExtra x;
             x.mu = B.mu;
-            pb_tile<kPbDose, TY, VY>(P.g, B.f, B.t, B.wet, bx, by, k, acc, x);
+            pb_tile<kPbDose, TY, VY>(P.g, B.f, B.t, B.wet, bx, by, bz, acc, x);
         }
-        const int i = bx * kPbThreadsX + threadIdx.x;
 #pragma unroll
         for (int v = 0; v < VY; ++v) {
-            const int j = by * (TY * VY) + threadIdx.y + v * TY;
-            const long long u = (long long)i + (long long)P.g.nx * (j + (long long)P.g.ny * k);
-            if (i < P.g.nx && j < P.g.ny && DC_IN_BOUNDS(u, P.g.n(), 23)) P.dose[u] = acc[v];
+            const int3 q = pb_tile_voxel<TY, VY>(bx, by, bz, v);
+            const long long u = (long long)q.x + (long long)P.g.nx * (q.y + (long long)P.g.ny * q.z);
+            if (q.x < P.g.nx && q.y < P.g.ny && q.z < P.g.nz && DC_IN_BOUNDS(u, P.g.n(), 23)) P.dose[u] = acc[v];
         }
     }
 }
@@ -762,8 +792,8 @@ static void pb_launch(DeviceContext &ctx, const char *name, const Grid &g, const
     static bool attr_set[64] = {false};
     pb_attr(pb_kernel<kMode, kPbThreadsY, kPbVoxY>, smem, ctx.device, attr_set);
     dim3 block(kPbThreadsX, kPbThreadsY, 1);
-    dim3 grid((unsigned)((g.nx + kPbThreadsX - 1) / kPbThreadsX),
-              (unsigned)((g.ny + kPbThreadsY * kPbVoxY - 1) / (kPbThreadsY * kPbVoxY)), (unsigned)g.nz);
+    const int3 nt = pb_tiles<kPbThreadsY, kPbVoxY>(g);
+    dim3 grid((unsigned)nt.x, (unsigned)nt.y, (unsigned)nt.z);
     KernelTimer kt(ctx, name, s);
     pb_kernel<kMode, kPbThreadsY, kPbVoxY><<<grid, block, smem, s>>>(g, f, t, wet_s, dose, x);
     check_launch(name);
@@ -820,6 +850,17 @@ int pencil_beam_batch_variants() { return (int)(sizeof(kPbVariants) / sizeof(kPb
 void pencil_beam_batch_tile(int variant, int *ty, int *vy) {
     *ty = kPbVariants[variant][0];
     *vy = kPbVariants[variant][1];
+}
+long long pencil_beam_batch_tiles(int variant, const Grid &g) {
+    int3 n{};
+    switch (variant) {
+        case 0: n = pb_tiles<8, 2>(g); break;
+        case 1: n = pb_tiles<4, 2>(g); break;
+        case 2: n = pb_tiles<8, 1>(g); break;
+        case 3: n = pb_tiles<4, 4>(g); break;
+        default: throw Error(DC_ERR_VALUE, "unknown pencil-beam tile variant");
+    }
+    return (long long)n.x * n.y * n.z;
 }
 
 template <int TY, int VY>

@@ -98,6 +98,57 @@ __device__ float march_from(const Grid &g, const Frame &f, cudaTextureObject_t d
     return wet_sum;
 }
 
+// Exit of the ray from p along u out of the texture box: the distance t_exit,
+// the exit face's |cos| to the ray and its voxel spacing.
+struct RayExit {
+    float t_exit, cos_face, sp_face;
+};
+__device__ __forceinline__ RayExit ray_exit(const Grid &g, const Frame &f, float3 p, float3 u) {
+    RayExit e{3.0e38f, 1.0f, g.sx};
+    const float lo[3] = {-0.5f * g.sx - f.isox, -0.5f * g.sy - f.isoy, -0.5f * g.sz - f.isoz};
+    const float hi[3] = {((float)g.nx - 0.5f) * g.sx - f.isox, ((float)g.ny - 0.5f) * g.sy - f.isoy,
+                         ((float)g.nz - 0.5f) * g.sz - f.isoz};
+    const float pp[3] = {p.x, p.y, p.z}, uu[3] = {u.x, u.y, u.z}, ss[3] = {g.sx, g.sy, g.sz};
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        if (uu[a] == 0.0f) continue;
+        const float t = ((uu[a] > 0.0f ? hi[a] : lo[a]) - pp[a]) / uu[a];
+        if (t < e.t_exit) {
+            e.t_exit = t;
+            e.cos_face = fabsf(uu[a]);
+            e.sp_face = ss[a];
+        }
+    }
+    return e;
+}
+
+// The reference loop's sample count K: the first t = 0, 1, 2, ... whose
+// sample is outside the texture box.  Each texture coordinate is a monotone
+// function of t (fma and the rounding are monotone), so the inside samples
+// form a prefix, and K is the analytic exit distance corrected by the
+// reference's own float test at the candidates.  Returns -1 when four steps
+// either way do not settle it.
+__device__ __forceinline__ int exact_sample_count(const Grid &g, const Frame &f, float3 p, float3 u, float t_exit) {
+    int K = (int)fminf(floorf(t_exit), 1.0e6f) + 1;
+    if (K < 1) K = 1;
+    for (int it = 0; it < 4 && K > 1 && !march_inside(g, f, p, u, (float)(K - 1)); ++it) --K;
+    for (int it = 0; it < 4 && march_inside(g, f, p, u, (float)K); ++it) ++K;
+    if (!(march_inside(g, f, p, u, (float)(K - 1)) || K == 1) || march_inside(g, f, p, u, (float)K)) return -1;
+    return K;
+}
+
+// The reference's march over its K inside samples, summed in its order, with
+// the loop unrolled so that several texture fetches are in flight at once
+// (the fetch addresses do not depend on the sum).  Equal to march_from from
+// t = 0 bit for bit.
+__device__ __forceinline__ float march_count(const Grid &g, const Frame &f, cudaTextureObject_t density, float3 p,
+                                             float3 u, int K) {
+    float wet_sum = -0.05f;
+#pragma unroll 8
+    for (int t = 0; t < K; ++t) wet_sum = fmaf(march_sample(g, f, density, p, u, (float)t), 0.1f, wet_sum);
+    return wet_sum;
+}
+
 }  // namespace
 
 __global__ void __launch_bounds__(1024) xray_lattice_kernel(Grid g, Frame f, XrayLattice L,
@@ -165,31 +216,15 @@ __global__ void __launch_bounds__(128) xray_voxel_kernel(Grid g, Frame f, XrayLa
 
     bool exact = false;
     float wet_sum = 0.0f;
-    // --- exit distance along u from the texture box [lo, hi) per axis, and the exit face
-    float t_exit = 3.0e38f, cos_face = 1.0f, sp_face = g.sx;
-    {
-        const float lo[3] = {-0.5f * g.sx - f.isox, -0.5f * g.sy - f.isoy, -0.5f * g.sz - f.isoz};
-        const float hi[3] = {((float)g.nx - 0.5f) * g.sx - f.isox, ((float)g.ny - 0.5f) * g.sy - f.isoy,
-                             ((float)g.nz - 0.5f) * g.sz - f.isoz};
-        const float pp[3] = {p.x, p.y, p.z}, uu[3] = {u.x, u.y, u.z}, ss[3] = {g.sx, g.sy, g.sz};
-#pragma unroll
-        for (int a = 0; a < 3; ++a) {
-            if (uu[a] == 0.0f) continue;
-            const float t = ((uu[a] > 0.0f ? hi[a] : lo[a]) - pp[a]) / uu[a];
-            if (t < t_exit) {
-                t_exit = t;
-                cos_face = fabsf(uu[a]);
-                sp_face = ss[a];
-            }
-        }
+    // --- exit distance along u from the texture box [lo, hi) per axis, the
+    // exit face, and the exact sample count K of the reference's loop
+    const RayExit ex = ray_exit(g, f, p, u);
+    const float cos_face = ex.cos_face, sp_face = ex.sp_face;
+    int K = exact_sample_count(g, f, p, u, ex.t_exit);
+    if (K < 0) {
+        exact = true;
+        K = 1;
     }
-    // --- the exact sample count K of the reference's loop: first t = 0,1,2,..
-    // whose sample is outside (the inside samples are a prefix)
-    int K = (int)fminf(floorf(t_exit), 1.0e6f) + 1;
-    if (K < 1) K = 1;
-    for (int it = 0; it < 4 && K > 1 && !march_inside(g, f, p, u, (float)(K - 1)); ++it) --K;
-    for (int it = 0; it < 4 && march_inside(g, f, p, u, (float)K); ++it) ++K;
-    if (!(march_inside(g, f, p, u, (float)(K - 1)) || K == 1) || march_inside(g, f, p, u, (float)K)) exact = true;
 
     // --- exact boundary samples: the blend zone of the texture filter plus the
     // spread of exit distances between the voxel's ray and its lattice rays
@@ -253,7 +288,7 @@ __global__ void __launch_bounds__(128) xray_voxel_kernel(Grid g, Frame f, XrayLa
     }
     if (!exact) {
         if (mt == K) {
-            wet_sum = march_from(g, f, density, p, u, 0.0f, -0.05f);  // the reference's own sum
+            wet_sum = march_count(g, f, density, p, u, K);  // the reference's own sum
         } else {
             float tail = 0.0f;
             for (int t = K - mt; t < K; ++t) tail += march_sample(g, f, density, p, u, (float)t);
@@ -264,7 +299,7 @@ __global__ void __launch_bounds__(128) xray_voxel_kernel(Grid g, Frame f, XrayLa
             // e.g. through air, join the list).
             if (!(wet_sum >= L.wet_exact)) {
                 if (K <= kInlineMarch)
-                    wet_sum = march_from(g, f, density, p, u, 0.0f, -0.05f);
+                    wet_sum = march_count(g, f, density, p, u, K);
                 else
                     exact = true;
             }
@@ -304,7 +339,8 @@ __global__ void __launch_bounds__(128) xray_fallback_kernel(Grid g, Frame f, cud
         const int i = rem - j * g.nx;
         const float3 p = voxel_xyz(g, f, i, j, k);
         const float3 u = unit_to_source(f, p);
-        wet[v] = march_from(g, f, density, p, u, 0.0f, -0.05f);
+        const int K = exact_sample_count(g, f, p, u, ray_exit(g, f, p, u).t_exit);
+        wet[v] = K >= 0 ? march_count(g, f, density, p, u, K) : march_from(g, f, density, p, u, 0.0f, -0.05f);
     }
 }
 

@@ -59,7 +59,14 @@ def test_batch_anisotropic_plan_matches_oracle(batch):
         w = b.wets[bid].cpu().numpy()
         o, _ = oracle.proton_dose(w, sp, grid.origin, bm.iso, bm.gantry_angle, bm.couch_angle, model, bm.spot_list)
         ref += o
-    assert dose_diff(b.doses[pid].cpu().numpy(), ref) <= 1e-3
+    d = b.doses[pid].cpu().numpy()
+    # the distance to the spot axis is taken as |ray x t|^2 / |t|^2, free of
+    # the cancellation in |ray|^2 - (t.ray)^2 / |t|^2, so float tracks FP64
+    # closely on every voxel, not only above 10 % of the maximum
+    print("\nbatch plan vs FP64 oracle: %.2e of Dmax above 10 %%, %.2e on every voxel"
+          % (dose_diff(d, ref), dose_diff(d, ref, thresh=0.0)))
+    assert dose_diff(d, ref) <= 1e-4
+    assert dose_diff(d, ref, thresh=0.0) <= 1e-4
 
 
 def test_batch_influence_matrix_equals_the_per_beam_matrix(batch):

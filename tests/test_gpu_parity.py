@@ -147,7 +147,12 @@ def test_proton_small_workload_vs_oracle(dk):
     sp = np.asarray(rl.spacing)[[0, 0, 0]]
     d_o, _ = oracle.proton_dose(w, sp, rl.origin, beam.iso, beam.gantry_angle, beam.couch_angle, model,
                                 beam.spot_list)
-    assert dose_diff(d, d_o) <= 1e-3
+    # float against FP64 on every voxel: the axis distance is computed without
+    # the reference's cancellation (|ray x t|^2 / |t|^2)
+    print("\nproton 96^3 vs FP64 oracle: %.2e of Dmax above 10 %%, %.2e on every voxel"
+          % (dose_diff(d, d_o), dose_diff(d, d_o, thresh=0.0)))
+    assert dose_diff(d, d_o) <= 1e-4
+    assert dose_diff(d, d_o, thresh=0.0) <= 1e-4
 
 
 def test_photon_small_workload_vs_oracle_and_reference(dk, imrt_plan):
