@@ -480,7 +480,7 @@ void upload_host_volume(DeviceContext &ctx, const float *src, int nz, int ny, in
         enqueue(src, 0, nz);
         return;
     }
-    constexpr size_t kSlab = 2u << 20;  // bytes per pinned slab (at least one plane)
+    constexpr size_t kSlab = 1u << 20;  // bytes per pinned slab (at least one plane)
     const int zc = (int)std::max<size_t>(1, kSlab / plane);
     int slot = 0;
     for (int z0 = 0; z0 < nz; z0 += zc, slot = (slot + 1) % DeviceContext::kStageSlots) {
