@@ -22,7 +22,8 @@ struct XrayLattice {
     int na, nb, m0, nm;
     float sad;         // source distance (mm)
     float tau;         // largest spread of the four rays' sums interpolated (mm x density)
-    float wet_exact;   // WET (cm) below which a voxel's depth is marched exactly
+    float wet_exact;   // WET (cm) below which a voxel's depth is marched exactly ...
+    float tau_shallow; // ... where its four lattice rays' sums spread by more than this (mm x density)
     float3 src;        // source, image frame relative to the isocentre
     float3 ex, ey, ez; // head-frame axes in the image frame
 };
@@ -33,7 +34,8 @@ bool plan_xray_lattice(const Grid &g, const Frame &f, XrayLattice &L);
 // march for the voxels the lattice cannot serve (listed in list/n_list, which
 // need room for every voxel); the plain march when the lattice does not apply.
 // Voxels whose WET comes out below `wet_exact` (cm) are marched exactly too
-// (+infinity: the plain march for every voxel).  `stats` (device word, or
+// where their lattice rays disagree (+infinity: the plain march for every
+// voxel).  `stats` (device word, or
 // null) receives the number of voxels marched from the list (0xffffffff when
 // the lattice did not apply).
 void launch_xray_depth(DeviceContext &ctx, const Grid &g, const Frame &f, cudaTextureObject_t density, float *wet,

@@ -493,14 +493,17 @@ static float electron_exact_wet(const PhotonParams &P) {
 
 void photon_head_fork(DeviceContext &ctx, const Grid &g, const Frame &f, const PhotonParams &P, cudaStream_t s) {
     float4 *head = static_cast<float4 *>(ctx.head.ensure((size_t)g.n() * sizeof(float4)));
+    // With the kernel profiler on, the head factors run on s itself, so that
+    // no kernel's timed interval includes another's share of the SMs.
+    const cudaStream_t hs = ctx.profiling && !DeviceContext::capturing(s) ? s : ctx.side;
     DC_CUDA(cudaEventRecord(ctx.fork_ev, s));
-    DC_CUDA(cudaStreamWaitEvent(ctx.side, ctx.fork_ev, 0));
+    DC_CUDA(cudaStreamWaitEvent(hs, ctx.fork_ev, 0));
     {
-        KernelTimer kt(ctx, "head", ctx.side);
-        head_kernel<<<vol_grid(g), dim3(32, 4, 1), 0, ctx.side>>>(g, f, P, head);
+        KernelTimer kt(ctx, "head", hs);
+        head_kernel<<<vol_grid(g), dim3(32, 4, 1), 0, hs>>>(g, f, P, head);
         check_launch("head_kernel");
     }
-    DC_CUDA(cudaEventRecord(ctx.join_ev, ctx.side));
+    DC_CUDA(cudaEventRecord(ctx.join_ev, hs));
     ctx.head_forked = true;
 }
 

@@ -77,7 +77,10 @@ def proton_small(seed=0, shape=(96, 96, 96), spacing=2.0, **beam_kw):
 
 
 def photon_phantom(shape=(128, 128, 128), spacing=2.5, seed=0, lung_mm=(60.0, 60.0, 40.0),
-                   bone_mm=20.0) -> IMRTDoseGrid:
+                   bone_mm=20.0, body_mm=None) -> IMRTDoseGrid:
+    """Water with a lung block and a bone cube at seeded offsets; with
+    ``body_mm`` = (a, b, c) semi-axes (x, y, z), the water is an ellipsoidal
+    body centred in the volume and everything outside it is air (-1000 HU)."""
     rng = np.random.default_rng(seed)
     nz, ny, nx = shape
     grid = IMRTDoseGrid()
@@ -92,6 +95,9 @@ def photon_phantom(shape=(128, 128, 128), spacing=2.5, seed=0, lung_mm=(60.0, 60
     hu[(np.abs(X - c[0]) < lx / 2) & (np.abs(Y - c[1]) < ly / 2) & (np.abs(Z - c[2]) < lz / 2)] = -750.0
     c = rng.uniform(-0.2, 0.2, size=3) * ext
     hu[(np.abs(X - c[0]) < bone_mm / 2) & (np.abs(Y - c[1]) < bone_mm / 2) & (np.abs(Z - c[2]) < bone_mm / 2)] = 1200.0
+    if body_mm is not None:
+        a, b, cz = body_mm
+        hu[(X / a) ** 2 + (Y / b) ** 2 + (Z / cz) ** 2 > 1.0] = -1000.0
     grid.HU = hu
     return grid
 
