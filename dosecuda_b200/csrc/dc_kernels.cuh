@@ -21,7 +21,10 @@ struct XrayLattice {
     float a0, b0, pa, inv_pa;
     int na, nb, m0, nm;
     float sad;         // source distance (mm)
-    float tau;         // largest spread of the four rays' sums interpolated (mm x density)
+    float tau;         // largest spread of the four rays' sums interpolated (mm x density), ...
+    float rho_floor;   // ... weighed by the voxel's own density, at least this
+    float tau_big;     // largest weighed spread accepted where ...
+    float tau_curv;    // ... the 4 x 4 rays' second-difference error estimate is below this
     float wet_exact;   // WET (cm) below which a voxel's depth is marched exactly ...
     float tau_shallow; // ... where its four lattice rays' sums spread by more than this (mm x density)
     float3 src;        // source, image frame relative to the isocentre

@@ -28,9 +28,12 @@
 //     last m samples next to the volume's boundary, where the texture filter
 //     blends in the border value and neighbouring rays leave the volume at
 //     different distances, are fetched exactly.  Where the four rays' sums
-//     differ by more than `tau` (a density edge running along the beam, the
-//     volume's side faces) or the voxel falls outside the lattice, the voxel
-//     joins a list instead.
+//     differ by more than `tau` divided by the voxel's own density (the CCCS
+//     weighs a voxel's TERMA by its density, so an air voxel's WET matters
+//     little), and the second differences of the 4 x 4 rays around the cell
+//     do not show the variation to be near-linear (a density edge running
+//     along the beam, the volume's side faces), or the voxel falls outside
+//     the lattice, the voxel joins a list instead.
 //  3. xray_fallback_kernel: the reference's march, exactly, for the listed
 //     voxels (a persistent grid over the device-side count).
 //
@@ -245,6 +248,7 @@ __global__ void __launch_bounds__(128) xray_voxel_kernel(Grid g, Frame f, XrayLa
     if (mt > K) mt = K;
 
     float S = 0.0f, spread = 0.0f;
+    bool shallow_unsure = false;  // the lattice's sum is not known to 0.001 cm of WET
     if (!exact && K > mt) {
         const float3 h = image_to_head<true>(f, p);
         const float den = L.sad - h.z;
@@ -264,11 +268,9 @@ __global__ void __launch_bounds__(128) xray_voxel_kernel(Grid g, Frame f, XrayLa
             const float wa = fa - xa, wb = fb - xb, fh = x_hi - n_hi, fl = x_lo - n_lo;
             const long long row = (long long)L.na * L.nb, total = row * L.nm;
             (void)total;  // read by the bounds checks of debug builds
-            float c[4];
-            float cmin = 3.0e38f, cmax = -3.0e38f;
-#pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                const long long r = (long long)(ib + (q >> 1)) * L.na + ia + (q & 1);
+            // the lattice ray (ra, rb)'s integral over the voxel's distance range
+            auto cval = [&](int ra, int rb) -> float {
+                const long long r = (long long)rb * L.na + ra;
                 const long long h0 = (long long)mh * row + r, l0 = (long long)ml * row + r;
                 float gh0 = 0.f, gh1 = 0.f, gl0 = 0.f, gl1 = 0.f;
                 if (DC_IN_BOUNDS(h0 + row, total, 41) && DC_IN_BOUNDS(h0, total, 41)) {
@@ -279,17 +281,68 @@ __global__ void __launch_bounds__(128) xray_voxel_kernel(Grid g, Frame f, XrayLa
                     gl0 = __ldg(G + l0);
                     gl1 = __ldg(G + l0 + row);
                 }
-                c[q] = fmaf(fh, gh1 - gh0, gh0) - fmaf(fl, gl1 - gl0, gl0);
+                return fmaf(fh, gh1 - gh0, gh0) - fmaf(fl, gl1 - gl0, gl0);
+            };
+            float c[4];
+            float cmin = 3.0e38f, cmax = -3.0e38f;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                c[q] = cval(ia + (q & 1), ib + (q >> 1));
                 cmin = fminf(cmin, c[q]);
                 cmax = fmaxf(cmax, c[q]);
             }
             spread = cmax - cmin;
-            if (spread > L.tau) {
+            // Bilinear interpolation is exact for a field varying linearly
+            // between the rays (a smooth gradient, e.g. behind a curved body
+            // surface), so where the corners spread more than tau the error is
+            // estimated from the second differences of the 4 x 4 rays around
+            // the cell: |f - bilinear| <= (|f_aa| + |f_bb|) / 8 for a quadratic
+            // field.  Computed on demand (+inf where the stencil leaves the
+            // lattice).
+            float est = -1.0f;
+            auto estimate = [&]() -> float {
+                if (est >= 0.0f) return est;
+                if (!(xa >= 1.0f && xb >= 1.0f && xa <= (float)(L.na - 3) && xb <= (float)(L.nb - 3))) {
+                    est = INFINITY;
+                    return est;
+                }
+                float sv[4][4];
+#pragma unroll
+                for (int rb = 0; rb < 4; ++rb)
+#pragma unroll
+                    for (int ra = 0; ra < 4; ++ra) {
+                        const bool corner = (rb == 1 || rb == 2) && (ra == 1 || ra == 2);
+                        sv[rb][ra] = corner ? c[(rb - 1) * 2 + (ra - 1)] : cval(ia - 1 + ra, ib - 1 + rb);
+                    }
+                float curv = 0.0f;
+#pragma unroll
+                for (int rb = 1; rb <= 2; ++rb)
+#pragma unroll
+                    for (int ra = 1; ra <= 2; ++ra) {
+                        const float d2a = sv[rb][ra - 1] - 2.0f * sv[rb][ra] + sv[rb][ra + 1];
+                        const float d2b = sv[rb - 1][ra] - 2.0f * sv[rb][ra] + sv[rb + 1][ra];
+                        curv = fmaxf(curv, fabsf(d2a) + fabsf(d2b));
+                    }
+                est = 0.125f * curv;
+                return est;
+            };
+            // The CCCS weights the TERMA sampled at a point by the density
+            // there (max(rho, 0.0012) x spacing), so a WET error enters the
+            // dose in proportion to the voxel's own density: the tests are
+            // weighed by it (water as before, bone stricter, air looser).
+            const float rho_v = tex3D<float>(density, (float)i + 0.5f, (float)j + 0.5f, (float)k + 0.5f);
+            const float wv = fmaxf(rho_v, L.rho_floor);
+            const bool ok = spread * wv <= L.tau || (spread * wv <= L.tau_big && estimate() * wv <= L.tau_curv);
+            if (!ok) {
                 exact = true;
             } else {
                 const float top = fmaf(wa, c[1] - c[0], c[0]);
                 const float bot = fmaf(wa, c[3] - c[2], c[2]);
                 S = fmaf(wb, bot - top, top);
+                // a voxel in the electron term's range needs its sum to 0.001
+                // cm; the second-difference estimate is not trusted that far
+                // (it missed voxel-scale structure on a body in air)
+                shallow_unsure = !(spread <= L.tau_shallow);
             }
         }
     } else if (!exact) {
@@ -307,8 +360,8 @@ __global__ void __launch_bounds__(128) xray_voxel_kernel(Grid g, Frame f, XrayLa
             // where the four lattice rays disagree by more than tau_shallow
             // the depth is marched exactly (short rays inline, long ones join
             // the list).  Where they agree (air, homogeneous tissue) the
-            // interpolation is kept: a voxel's sum lies within their spread.
-            if (!(wet_sum >= L.wet_exact) && !(spread <= L.tau_shallow)) {
+            // interpolation is kept.
+            if (!(wet_sum >= L.wet_exact) && shallow_unsure) {
                 if (K <= kInlineMarch)
                     wet_sum = march_count(g, f, density, p, u, K);
                 else
@@ -420,6 +473,9 @@ void launch_xray_depth(DeviceContext &ctx, const Grid &g, const Frame &f, cudaTe
         return;
     }
     L.wet_exact = wet_exact;
+    L.rho_floor = 0.05f;    // smallest density the spread test weighs by
+    L.tau_big = 3.0f;       // mm x density: largest spread accepted on a small second-difference estimate
+    L.tau_curv = 0.1f;      // mm x density: largest second-difference error estimate accepted
     L.tau_shallow = 0.01f;  // mm x density: 0.001 cm of WET, ~0.2 % of the electron term at the surface
     float *G = static_cast<float *>(lattice.ensure((size_t)L.na * L.nb * L.nm * sizeof(float)));
     {
