@@ -28,9 +28,9 @@
 //     last m samples next to the volume's boundary, where the texture filter
 //     blends in the border value and neighbouring rays leave the volume at
 //     different distances, are fetched exactly.  Where the four rays' sums
-//     differ by more than `tau` divided by the voxel's own density (the CCCS
-//     weighs a voxel's TERMA by its density, so an air voxel's WET matters
-//     little), and the second differences of the 4 x 4 rays around the cell
+//     differ by more than `tau` divided by the voxel's own density (capped at
+//     water's; the CCCS weighs a voxel's TERMA by its density, so an air
+//     voxel's WET matters little), and the second differences of the 4 x 4 rays around the cell
 //     do not show the variation to be near-linear (a density edge running
 //     along the beam, the volume's side faces), or the voxel falls outside
 //     the lattice, the voxel joins a list instead.
@@ -214,7 +214,7 @@ __global__ void __launch_bounds__(1024) xray_lattice_kernel(Grid g, Frame f, Xra
     }
 }
 
-__global__ void __launch_bounds__(128) xray_voxel_kernel(Grid g, Frame f, XrayLattice L, cudaTextureObject_t density,
+__global__ void __launch_bounds__(128, 10) xray_voxel_kernel(Grid g, Frame f, XrayLattice L, cudaTextureObject_t density,
                                                          const float *__restrict__ G, float *__restrict__ wet,
                                                          int *__restrict__ list, unsigned *__restrict__ n_list) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -328,11 +328,15 @@ __global__ void __launch_bounds__(128) xray_voxel_kernel(Grid g, Frame f, XrayLa
             };
             // The CCCS weights the TERMA sampled at a point by the density
             // there (max(rho, 0.0012) x spacing), so a WET error enters the
-            // dose in proportion to the voxel's own density: the tests are
-            // weighed by it (water as before, bone stricter, air looser).
-            const float rho_v = tex3D<float>(density, (float)i + 0.5f, (float)j + 0.5f, (float)k + 0.5f);
-            const float wv = fmaxf(rho_v, L.rho_floor);
-            const bool ok = spread * wv <= L.tau || (spread * wv <= L.tau_big && estimate() * wv <= L.tau_curv);
+            // dose in proportion to the voxel's own density: past tau the
+            // tests are weighed by it, capped at water's (lung and air looser,
+            // water and denser as tau), so the density is fetched only then.
+            bool ok = spread <= L.tau;
+            if (!ok) {
+                const float rho_v = tex3D<float>(density, (float)i + 0.5f, (float)j + 0.5f, (float)k + 0.5f);
+                const float wv = fmaxf(fminf(rho_v, 1.0f), L.rho_floor);
+                ok = spread * wv <= L.tau || (spread * wv <= L.tau_big && estimate() * wv <= L.tau_curv);
+            }
             if (!ok) {
                 exact = true;
             } else {

@@ -7,7 +7,7 @@ oracle.
 The lattice interpolates each voxel's density integral from the four lattice
 rays around its ray and marches exactly wherever they disagree by more than
 0.3 mm of unit density (0.03 cm of WET) divided by the voxel's own density
-(floor 0.05), so density-weighted TERMA moves by about the
+(capped at water's, floor 0.05), so density-weighted TERMA moves by about the
 attenuation of 0.03 cm of water at most, except on rays that graze a
 voxelised surface (a body in air), where a voxel's own ray can differ from
 all four by ~1 mm; voxels shallower than the electron
