@@ -157,7 +157,15 @@ int dc_release_device(int gpu_id);
  *                         interpolated per voxel, with the reference's exact
  *                         sample count, its boundary samples fetched exactly,
  *                         and the exact march wherever neighbouring lattice
- *                         rays disagree by more than 0.03 cm of WET.
+ *                         rays disagree by more than 0.03 cm of WET (weighed
+ *                         by the voxel's density, up to water's) without a
+ *                         near-linear variation between them, and for
+ *                         shallow voxels (electron contamination range)
+ *                         wherever they disagree by more than 0.001 cm.  An
+ *                         approximation: TERMA typically within 0.15 % of
+ *                         the march, up to ~1 % on rays grazing a voxelised
+ *                         body surface; the dose within 0.1 % of Dmax on the
+ *                         tested geometries.
  * Applies to calls enqueued after it returns; proton WET always uses the
  * march. */
 #define DC_DEPTH_MARCH 0
