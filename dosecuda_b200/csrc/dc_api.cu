@@ -61,11 +61,9 @@ void proton_raytrace_core(DeviceContext &ctx, const Grid &g, const Frame &f, flo
 }
 
 // Uploads the spot/layer tables (via pinned staging) and launches the pencil beam.
-// Layer and spot tables on the device (through a pinned staging slot) and
-// the layers' cut-off radii, enqueued on s.
-ProtonTables proton_tables(DeviceContext &ctx, const Grid &g, const Frame &f, const std::vector<LayerRec> &layers,
-                           const std::vector<SpotRec> &spots, const float *lut_d, const float *lut_s,
-                           const float *lut_i, int lut_len, cudaStream_t s) {
+void proton_spot_core(DeviceContext &ctx, const Grid &g, const Frame &f, const std::vector<LayerRec> &layers,
+                      const std::vector<SpotRec> &spots, const float *lut_d, const float *lut_s, const float *lut_i,
+                      int lut_len, const float *wet_s_dev, float *dose_dev, cudaStream_t s) {
     const size_t lb = layers.size() * sizeof(LayerRec);
     const size_t lb_al = (lb + 255) & ~(size_t)255;
     const size_t sb = spots.size() * sizeof(SpotRec);
@@ -88,13 +86,6 @@ ProtonTables proton_tables(DeviceContext &ctx, const Grid &g, const Frame &f, co
     t.lut_idds = lut_i;
     t.n_layers = (int)layers.size();
     t.lut_len = lut_len;
-    return t;
-}
-
-void proton_spot_core(DeviceContext &ctx, const Grid &g, const Frame &f, const std::vector<LayerRec> &layers,
-                      const std::vector<SpotRec> &spots, const float *lut_d, const float *lut_s, const float *lut_i,
-                      int lut_len, const float *wet_s_dev, float *dose_dev, cudaStream_t s) {
-    const ProtonTables t = proton_tables(ctx, g, f, layers, spots, lut_d, lut_s, lut_i, lut_len, s);
     launch_pencil_beam(ctx, g, f, t, wet_s_dev, dose_dev, s);
 }
 
@@ -310,26 +301,13 @@ int dc_proton_spot(int gpu_id, const float *wet, int nz, int ny, int nx, const f
         const size_t lb = (size_t)n_energies * lut_len * sizeof(float);
         const size_t lb_al = (lb + 255) & ~(size_t)255;
         char *lut = static_cast<char *>(ctx.lut.ensure(3 * lb_al));
+        if (!wet_direct) upload_host_volume(ctx, wet, nz, ny, nx, nullptr, wet_d, s);
         DC_CUDA(cudaMemcpyAsync(lut, lut_depths, lb, cudaMemcpyHostToDevice, s));
         DC_CUDA(cudaMemcpyAsync(lut + lb_al, lut_sigmas, lb, cudaMemcpyHostToDevice, s));
         DC_CUDA(cudaMemcpyAsync(lut + 2 * lb_al, lut_idds, lb, cudaMemcpyHostToDevice, s));
-        const ProtonTables t = proton_tables(ctx, g, f, layers, recs, reinterpret_cast<const float *>(lut),
-                                             reinterpret_cast<const float *>(lut + lb_al),
-                                             reinterpret_cast<const float *>(lut + 2 * lb_al), lut_len, s);
-        if (wet_direct) {
-            launch_pencil_beam(ctx, g, f, t, wet_direct, dose_d, s);
-        } else {
-            // A voxel's dose needs only its own WET: the pencil beam runs on
-            // the tiles whose planes have been uploaded while the host copies
-            // the next slab of a pageable WET.
-            const int depth = pencil_beam_tile_depth();
-            int done = 0;
-            upload_host_volume(ctx, wet, nz, ny, nx, nullptr, wet_d, s, [&](int planes) {
-                const int ready = planes >= nz ? (nz + depth - 1) / depth : planes / depth;
-                if (ready > done) launch_pencil_beam(ctx, g, f, t, wet_d, dose_d, s, nullptr, done, ready);
-                done = std::max(done, ready);
-            });
-        }
+        proton_spot_core(ctx, g, f, layers, recs, reinterpret_cast<const float *>(lut),
+                         reinterpret_cast<const float *>(lut + lb_al), reinterpret_cast<const float *>(lut + 2 * lb_al),
+                         lut_len, wet_direct ? wet_direct : wet_d, dose_d, s);
         if (!dose_direct) DC_CUDA(cudaMemcpyAsync(dose_out, dose_d, vb, cudaMemcpyDeviceToHost, s));
         ctx.end_call(s);
         DC_CUDA(cudaStreamSynchronize(s));

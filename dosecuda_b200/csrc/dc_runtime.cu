@@ -460,7 +460,7 @@ bool page_locked(const void *p) {
 }  // namespace
 
 void upload_host_volume(DeviceContext &ctx, const float *src, int nz, int ny, int nx, VolumeArray *arr, float *lin,
-                        cudaStream_t s, const std::function<void(int)> &on_slab) {
+                        cudaStream_t s) {
     const size_t plane = (size_t)nx * ny * sizeof(float);
     auto enqueue = [&](const float *from, int z0, int nzc) {
         if (arr) {
@@ -476,20 +476,12 @@ void upload_host_volume(DeviceContext &ctx, const float *src, int nz, int ny, in
                                     cudaMemcpyHostToDevice, s));
         }
     };
-    constexpr size_t kSlab = 1u << 20;  // bytes per pinned slab (at least one plane)
-    const int zc = (int)std::max<size_t>(1, kSlab / plane);
     if (page_locked(src)) {
-        if (!on_slab) {
-            enqueue(src, 0, nz);
-            return;
-        }
-        for (int z0 = 0; z0 < nz; z0 += zc) {
-            const int n = std::min(zc, nz - z0);
-            enqueue(src + (size_t)z0 * nx * ny, z0, n);
-            on_slab(z0 + n);
-        }
+        enqueue(src, 0, nz);
         return;
     }
+    constexpr size_t kSlab = 1u << 20;  // bytes per pinned slab (at least one plane)
+    const int zc = (int)std::max<size_t>(1, kSlab / plane);
     int slot = 0;
     for (int z0 = 0; z0 < nz; z0 += zc, slot = (slot + 1) % DeviceContext::kStageSlots) {
         const int n = std::min(zc, nz - z0);
@@ -499,7 +491,6 @@ void upload_host_volume(DeviceContext &ctx, const float *src, int nz, int ny, in
         host_copy_pool().copy(pin, reinterpret_cast<const char *>(src) + (size_t)z0 * plane, (size_t)n * plane);
         enqueue(reinterpret_cast<const float *>(pin), z0, n);
         DC_CUDA(cudaEventRecord(ctx.stage_ev[slot], s));
-        if (on_slab) on_slab(z0 + n);
     }
 }
 

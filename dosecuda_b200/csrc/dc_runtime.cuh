@@ -17,7 +17,6 @@
 
 #include "../../include/dosecuda.h"
 
-#include <functional>
 #include <map>
 #include <mutex>
 #include <new>
@@ -214,11 +213,8 @@ void *mapped_host_range(const void *host, size_t bytes);
 // is copied directly.  A pageable one is pipelined through the context's
 // pinned slabs: host threads copy slab c into a pinned buffer while the DMA
 // of slab c-1 runs, instead of the driver staging the whole volume serially.
-// With `on_slab`, the copy goes in slabs either way and on_slab(z) is called
-// after each slab's copy is enqueued, z = the planes enqueued so far, so that
-// the caller can enqueue work on those planes behind it.
 void upload_host_volume(DeviceContext &ctx, const float *src, int nz, int ny, int nx, VolumeArray *arr, float *lin,
-                        cudaStream_t s, const std::function<void(int)> &on_slab = nullptr);
+                        cudaStream_t s);
 
 // Throws Error(DC_ERR_CUDA) if the last launch failed.
 void check_launch(const char *kernel);
