@@ -322,7 +322,7 @@ struct UpArgs {
     int tiles_x, tiles_y, tiles_z;
 };
 
-template <int CC, int NT, int TY, int TZ>
+template <int CC, int NT, int TY, int TZ, int G>
 __global__ void __launch_bounds__(kThreads) conv_up_kernel(UpArgs a) {
     constexpr int WM = TY * TZ / 4;
     constexpr int S = CC / 2;  // k16 steps per tap
@@ -343,7 +343,12 @@ __global__ void __launch_bounds__(kThreads) conv_up_kernel(UpArgs a) {
     uint2 *sw = reinterpret_cast<uint2 *>(smem + TZ * TY * 16 * CC);
     load_tile<CC, kConv3, 16, TY, TZ>(smem, a.x + (size_t)nb * a.d * a.h * a.w * (CC * 8), CC * 8, 0, a.d, a.h,
                                       a.w, oz0, oy0, ox0, a.x);
-    stage_weights<S, NT>(sw, a.wt, 0, 8 * S, NT, 0);
+    // the CTA's taps: G groups of 8 / G taps over blockIdx.y (more CTAs on the
+    // coarse grids, where one CTA per tile leaves SMs idle)
+    constexpr int tpc = 8 / G;
+    static_assert(tpc * G == 8, "tap groups divide the 8 taps");
+    const int t0 = (int)blockIdx.y * tpc, t1 = t0 + tpc;
+    stage_weights<S, NT>(sw, a.wt, t0 * S, 8 * S, NT, 0);
     cp_async_commit();
 
     const int warp = tid >> 5, lane = tid & 31;
@@ -354,16 +359,16 @@ __global__ void __launch_bounds__(kThreads) conv_up_kernel(UpArgs a) {
     const int fd = 2 * a.d, fh = 2 * a.h, fw = 2 * a.w;
 
 #pragma unroll 1
-    for (int t = 0; t < 8; ++t) {
-        if (t + 1 < 8) {
-            stage_weights<S, NT>(sw + ((t + 1) & 1) * WORDS, a.wt, (t + 1) * S, 8 * S, NT, 0);
+    for (int t = t0; t < t1; ++t) {
+        if (t + 1 < t1) {
+            stage_weights<S, NT>(sw + ((t + 1 - t0) & 1) * WORDS, a.wt, (t + 1) * S, 8 * S, NT, 0);
             cp_async_commit();
             cp_async_wait_group<1>();
         } else {
             cp_async_wait_group<0>();
         }
         __syncthreads();
-        const uint2 *wb = sw + (t & 1) * WORDS + lane;
+        const uint2 *wb = sw + ((t - t0) & 1) * WORDS + lane;
         float acc[WM][NT][4];
 #pragma unroll
         for (int i = 0; i < WM; ++i)
@@ -919,19 +924,29 @@ void launch_gather(const GatherArgs &a0, int n, cudaStream_t s) {
     check_launch("conv_gather_kernel");
 }
 
+template <int CC, int NT, int TY, int TZ, int G>
+void launch_up_groups(const UpArgs &a, long long blocks, cudaStream_t s) {
+    const size_t smem = (size_t)TZ * TY * 16 * CC * 16 + 2 * (size_t)(CC / 2) * NT * 32 * sizeof(uint2);
+    auto k = conv_up_kernel<CC, NT, TY, TZ, G>;
+    set_smem(k, smem);
+    k<<<dim3((unsigned)blocks, (unsigned)G), kThreads, smem, s>>>(a);
+    check_launch("conv_up_kernel");
+}
+
 template <int CC, int NT, int TY, int TZ>
 void launch_up(const UpArgs &a0, int n, cudaStream_t s) {
     UpArgs a = a0;
     a.tiles_x = (a.w + 15) / 16;
     a.tiles_y = (a.h + TY - 1) / TY;
     a.tiles_z = (a.d + TZ - 1) / TZ;
-    const size_t smem = (size_t)TZ * TY * 16 * CC * 16 + 2 * (size_t)(CC / 2) * NT * 32 * sizeof(uint2);
-    auto k = conv_up_kernel<CC, NT, TY, TZ>;
-    set_smem(k, smem);
     const long long blocks = (long long)n * a.tiles_x * a.tiles_y * a.tiles_z;
     need(blocks < 0x7fffffffLL, "volume too large for the surrogate convolution");
-    k<<<(unsigned)blocks, kThreads, smem, s>>>(a);
-    check_launch("conv_up_kernel");
+    // tap groups: at least two waves of CTAs on the 148 SMs (measured: 16^3
+    // -> 32^3 128 -> 64 channels 54.6 -> 11.5 us, 32^3 -> 64^3 52.8 -> 21.3 us)
+    if (blocks >= 2 * 148) return launch_up_groups<CC, NT, TY, TZ, 1>(a, blocks, s);
+    if (2 * blocks >= 2 * 148) return launch_up_groups<CC, NT, TY, TZ, 2>(a, blocks, s);
+    if (4 * blocks >= 2 * 148) return launch_up_groups<CC, NT, TY, TZ, 4>(a, blocks, s);
+    return launch_up_groups<CC, NT, TY, TZ, 8>(a, blocks, s);
 }
 
 template <int MODE, int CCA, int NBT, int TY, int TZ>
@@ -1014,7 +1029,7 @@ void conv_gather(int mode, const bf16 *x, int n, int d, int h, int w, int cin, c
         if (cin == 8 && cout == 16) return launch_gather<kConv3, 1, 2, 8, 2>(a, n, s);
         if (cin == 16 && cout == 16) return launch_gather<kConv3, 2, 2, 8, 2>(a, n, s);
         if (cin == 32 && cout == 32) return launch_gather<kConv3, 4, 4, 8, 2>(a, n, s);
-        if (cin == 64 && cout == 64) return launch_gather<kConv3, 8, 8, 8, 2>(a, n, s);
+        if (cin == 64 && cout == 64) return launch_gather<kConv3, 8, 4, 8, 2>(a, n, s);      // 2 channel groups
         if (cin == 128 && cout == 128) return launch_gather<kConv3, 16, 4, 4, 2>(a, n, s);  // 4 channel groups
     } else {
         if (cin == 16 && cout == 32) return launch_gather<kDown2, 2, 4, 8, 2>(a, n, s);
