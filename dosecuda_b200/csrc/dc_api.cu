@@ -61,9 +61,11 @@ void proton_raytrace_core(DeviceContext &ctx, const Grid &g, const Frame &f, flo
 }
 
 // Uploads the spot/layer tables (via pinned staging) and launches the pencil beam.
-void proton_spot_core(DeviceContext &ctx, const Grid &g, const Frame &f, const std::vector<LayerRec> &layers,
-                      const std::vector<SpotRec> &spots, const float *lut_d, const float *lut_s, const float *lut_i,
-                      int lut_len, const float *wet_s_dev, float *dose_dev, cudaStream_t s) {
+// Layer and spot tables on the device (through a pinned staging slot) and
+// the layers' cut-off radii, enqueued on s.
+ProtonTables proton_tables(DeviceContext &ctx, const Grid &g, const Frame &f, const std::vector<LayerRec> &layers,
+                           const std::vector<SpotRec> &spots, const float *lut_d, const float *lut_s,
+                           const float *lut_i, int lut_len, cudaStream_t s) {
     const size_t lb = layers.size() * sizeof(LayerRec);
     const size_t lb_al = (lb + 255) & ~(size_t)255;
     const size_t sb = spots.size() * sizeof(SpotRec);
@@ -86,6 +88,13 @@ void proton_spot_core(DeviceContext &ctx, const Grid &g, const Frame &f, const s
     t.lut_idds = lut_i;
     t.n_layers = (int)layers.size();
     t.lut_len = lut_len;
+    return t;
+}
+
+void proton_spot_core(DeviceContext &ctx, const Grid &g, const Frame &f, const std::vector<LayerRec> &layers,
+                      const std::vector<SpotRec> &spots, const float *lut_d, const float *lut_s, const float *lut_i,
+                      int lut_len, const float *wet_s_dev, float *dose_dev, cudaStream_t s) {
+    const ProtonTables t = proton_tables(ctx, g, f, layers, spots, lut_d, lut_s, lut_i, lut_len, s);
     launch_pencil_beam(ctx, g, f, t, wet_s_dev, dose_dev, s);
 }
 
@@ -301,13 +310,35 @@ int dc_proton_spot(int gpu_id, const float *wet, int nz, int ny, int nx, const f
         const size_t lb = (size_t)n_energies * lut_len * sizeof(float);
         const size_t lb_al = (lb + 255) & ~(size_t)255;
         char *lut = static_cast<char *>(ctx.lut.ensure(3 * lb_al));
-        if (!wet_direct) upload_host_volume(ctx, wet, nz, ny, nx, nullptr, wet_d, s);
         DC_CUDA(cudaMemcpyAsync(lut, lut_depths, lb, cudaMemcpyHostToDevice, s));
         DC_CUDA(cudaMemcpyAsync(lut + lb_al, lut_sigmas, lb, cudaMemcpyHostToDevice, s));
         DC_CUDA(cudaMemcpyAsync(lut + 2 * lb_al, lut_idds, lb, cudaMemcpyHostToDevice, s));
-        proton_spot_core(ctx, g, f, layers, recs, reinterpret_cast<const float *>(lut),
-                         reinterpret_cast<const float *>(lut + lb_al), reinterpret_cast<const float *>(lut + 2 * lb_al),
-                         lut_len, wet_direct ? wet_direct : wet_d, dose_d, s);
+        const ProtonTables t = proton_tables(ctx, g, f, layers, recs, reinterpret_cast<const float *>(lut),
+                                             reinterpret_cast<const float *>(lut + lb_al),
+                                             reinterpret_cast<const float *>(lut + 2 * lb_al), lut_len, s);
+        if (wet_direct) {
+            launch_pencil_beam(ctx, g, f, t, wet_direct, dose_d, s);
+        } else {
+            // A voxel's dose needs only its own WET: the pencil beam runs on
+            // the tiles whose planes have been uploaded, on the side stream,
+            // while the next slab is copied on s.  Each launch waits on an
+            // event recorded behind its slab's copy (a wait takes the event's
+            // state when enqueued, so the one event is re-recorded per slab);
+            // s joins the side stream at the end.
+            const int depth = pencil_beam_tile_depth();
+            int done = 0;
+            upload_host_volume(ctx, wet, nz, ny, nx, nullptr, wet_d, s, [&](int planes) {
+                const int ready = planes >= nz ? (nz + depth - 1) / depth : planes / depth;
+                if (ready > done) {
+                    DC_CUDA(cudaEventRecord(ctx.fork_ev, s));
+                    DC_CUDA(cudaStreamWaitEvent(ctx.side, ctx.fork_ev, 0));
+                    launch_pencil_beam(ctx, g, f, t, wet_d, dose_d, ctx.side, nullptr, done, ready);
+                }
+                done = std::max(done, ready);
+            });
+            DC_CUDA(cudaEventRecord(ctx.join_ev, ctx.side));
+            DC_CUDA(cudaStreamWaitEvent(s, ctx.join_ev, 0));
+        }
         if (!dose_direct) DC_CUDA(cudaMemcpyAsync(dose_out, dose_d, vb, cudaMemcpyDeviceToHost, s));
         ctx.end_call(s);
         DC_CUDA(cudaStreamSynchronize(s));

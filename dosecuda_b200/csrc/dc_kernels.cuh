@@ -100,6 +100,9 @@ struct PbExtra {
     const int *list = nullptr;
     int n_list = 0;
     float *list_out = nullptr;
+    // image-tile modes: the tiles along z launched, [tile_z0, tile_z1) (tile_z1
+    // < 0: to the last)
+    int tile_z0 = 0, tile_z1 = -1;
 };
 
 enum PbMode { kPbDose = 0, kPbAdjoint = 1, kPbSpotMax = 2, kPbCount = 3, kPbFill = 4 };
@@ -122,7 +125,11 @@ void build_proton_tables(const float *spots, int n_spots, const float *dvp, int 
                          std::vector<SpotRec> &spot_recs);
 
 void launch_pencil_beam(DeviceContext &ctx, const Grid &g, const Frame &f, const ProtonTables &t,
-                        const float *wet_s, float *dose, cudaStream_t s, const float *mu_dev = nullptr);
+                        const float *wet_s, float *dose, cudaStream_t s, const float *mu_dev = nullptr,
+                        int tile_z0 = 0, int tile_z1 = -1);
+// Voxels along z per tile of the single-beam pencil-beam kernel: tiles
+// [z0, z1) cover planes [z0 * depth, z1 * depth).
+int pencil_beam_tile_depth();
 // Dose (x.list_out) or adjoint (x.grad_dose compact, x.grad_mu) of the voxels
 // in x.list only; mode kPbDose or kPbAdjoint.
 void launch_pencil_beam_list(DeviceContext &ctx, int mode, const Grid &g, const Frame &f, const ProtonTables &t,

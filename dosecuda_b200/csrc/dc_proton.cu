@@ -702,11 +702,12 @@ __global__ void __launch_bounds__(kPbThreadsX *TY, pb_min_ctas(TY, 4))
     float acc[VY];
 #pragma unroll
     for (int v = 0; v < VY; ++v) acc[v] = 0.0f;
-    pb_tile<kMode, TY, VY>(g, f, t, wet_s, blockIdx.x, blockIdx.y, blockIdx.z, acc, x);
+    const int bz = (int)blockIdx.z + x.tile_z0;
+    pb_tile<kMode, TY, VY>(g, f, t, wet_s, blockIdx.x, blockIdx.y, bz, acc, x);
     if (kMode == kPbDose) {
 #pragma unroll
         for (int v = 0; v < VY; ++v) {
-            const int3 q = pb_tile_voxel<TY, VY>(blockIdx.x, blockIdx.y, blockIdx.z, v);
+            const int3 q = pb_tile_voxel<TY, VY>(blockIdx.x, blockIdx.y, bz, v);
             const long long u = (long long)q.x + (long long)g.nx * (q.y + (long long)g.ny * q.z);
             if (q.x < g.nx && q.y < g.ny && q.z < g.nz && DC_IN_BOUNDS(u, g.n(), 20)) dose[u] = acc[v];
         }
@@ -793,18 +794,26 @@ static void pb_launch(DeviceContext &ctx, const char *name, const Grid &g, const
     pb_attr(pb_kernel<kMode, kPbThreadsY, kPbVoxY>, smem, ctx.device, attr_set);
     dim3 block(kPbThreadsX, kPbThreadsY, 1);
     const int3 nt = pb_tiles<kPbThreadsY, kPbVoxY>(g);
-    dim3 grid((unsigned)nt.x, (unsigned)nt.y, (unsigned)nt.z);
+    // tiles x.tile_z0 .. tile_z1 - 1 along z (all of them by default)
+    const int z1 = x.tile_z1 < 0 ? nt.z : std::min(x.tile_z1, nt.z);
+    if (x.tile_z0 < 0 || x.tile_z0 >= z1) return;
+    dim3 grid((unsigned)nt.x, (unsigned)nt.y, (unsigned)(z1 - x.tile_z0));
     KernelTimer kt(ctx, name, s);
     pb_kernel<kMode, kPbThreadsY, kPbVoxY><<<grid, block, smem, s>>>(g, f, t, wet_s, dose, x);
     check_launch(name);
 }
 
 void launch_pencil_beam(DeviceContext &ctx, const Grid &g, const Frame &f, const ProtonTables &t,
-                        const float *wet_s, float *dose, cudaStream_t s, const float *mu_dev) {
+                        const float *wet_s, float *dose, cudaStream_t s, const float *mu_dev, int tile_z0,
+                        int tile_z1) {
     PbExtra x;
     x.mu = mu_dev;
+    x.tile_z0 = tile_z0;
+    x.tile_z1 = tile_z1;
     pb_launch<kPbDose>(ctx, "pencil_beam", g, f, t, wet_s, dose, x, s);
 }
+
+int pencil_beam_tile_depth() { return PbTileShape<kPbThreadsY, kPbVoxY>::z; }
 
 void launch_pencil_beam_mode(DeviceContext &ctx, int mode, const Grid &g, const Frame &f, const ProtonTables &t,
                              const float *wet_s, const PbExtra &x, cudaStream_t s) {

@@ -199,6 +199,7 @@ DeviceContext::DeviceContext(int dev) : device(dev) {
     DC_CUDA(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking));
     DC_CUDA(cudaEventCreateWithFlags(&fork_ev, cudaEventDisableTiming));
     DC_CUDA(cudaEventCreateWithFlags(&join_ev, cudaEventDisableTiming));
+    DC_CUDA(cudaEventCreateWithFlags(&side_idle, cudaEventDisableTiming));
     for (auto &e : pin_ev) DC_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     for (auto &e : stage_ev) DC_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     DC_CUDA(cudaEventCreateWithFlags(&last_use, cudaEventDisableTiming));
@@ -212,7 +213,13 @@ bool DeviceContext::capturing(cudaStream_t s) {
 
 void DeviceContext::begin_call(cudaStream_t s) {
     head_forked = false;  // a fork left by a call that failed midway is never joined
-    if (!capturing(s)) DC_CUDA(cudaStreamWaitEvent(s, last_use, 0));
+    if (!capturing(s)) {
+        DC_CUDA(cudaStreamWaitEvent(s, last_use, 0));
+        // work a call that failed midway left on the side stream is ordered
+        // before this call's use of the shared scratch
+        DC_CUDA(cudaEventRecord(side_idle, side));
+        DC_CUDA(cudaStreamWaitEvent(s, side_idle, 0));
+    }
 }
 
 void DeviceContext::end_call(cudaStream_t s) {
@@ -259,7 +266,7 @@ void DeviceContext::release_all() {
     }
     if (last_use) cudaEventDestroy(last_use);
     last_use = nullptr;
-    for (cudaEvent_t *e : {&fork_ev, &join_ev}) {
+    for (cudaEvent_t *e : {&fork_ev, &join_ev, &side_idle}) {
         if (*e) cudaEventDestroy(*e);
         *e = nullptr;
     }
@@ -460,7 +467,7 @@ bool page_locked(const void *p) {
 }  // namespace
 
 void upload_host_volume(DeviceContext &ctx, const float *src, int nz, int ny, int nx, VolumeArray *arr, float *lin,
-                        cudaStream_t s) {
+                        cudaStream_t s, const std::function<void(int)> &on_slab) {
     const size_t plane = (size_t)nx * ny * sizeof(float);
     auto enqueue = [&](const float *from, int z0, int nzc) {
         if (arr) {
@@ -476,12 +483,20 @@ void upload_host_volume(DeviceContext &ctx, const float *src, int nz, int ny, in
                                     cudaMemcpyHostToDevice, s));
         }
     };
-    if (page_locked(src)) {
-        enqueue(src, 0, nz);
-        return;
-    }
     constexpr size_t kSlab = 1u << 20;  // bytes per pinned slab (at least one plane)
     const int zc = (int)std::max<size_t>(1, kSlab / plane);
+    if (page_locked(src)) {
+        if (!on_slab) {
+            enqueue(src, 0, nz);
+            return;
+        }
+        for (int z0 = 0; z0 < nz; z0 += zc) {
+            const int n = std::min(zc, nz - z0);
+            enqueue(src + (size_t)z0 * nx * ny, z0, n);
+            on_slab(z0 + n);
+        }
+        return;
+    }
     int slot = 0;
     for (int z0 = 0; z0 < nz; z0 += zc, slot = (slot + 1) % DeviceContext::kStageSlots) {
         const int n = std::min(zc, nz - z0);
@@ -491,6 +506,7 @@ void upload_host_volume(DeviceContext &ctx, const float *src, int nz, int ny, in
         host_copy_pool().copy(pin, reinterpret_cast<const char *>(src) + (size_t)z0 * plane, (size_t)n * plane);
         enqueue(reinterpret_cast<const float *>(pin), z0, n);
         DC_CUDA(cudaEventRecord(ctx.stage_ev[slot], s));
+        if (on_slab) on_slab(z0 + n);
     }
 }
 

@@ -17,6 +17,7 @@
 
 #include "../../include/dosecuda.h"
 
+#include <functional>
 #include <map>
 #include <mutex>
 #include <new>
@@ -112,7 +113,7 @@ class DeviceContext {
     // Side stream for work that runs beside a call's own stream: forked after
     // fork_ev (recorded on the call's stream), joined through join_ev.
     cudaStream_t side = nullptr;
-    cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
+    cudaEvent_t fork_ev = nullptr, join_ev = nullptr, side_idle = nullptr;
     bool head_forked = false;  // photon head factors enqueued on `side`, not yet joined
 
     DeviceBuffer wet_raw;     // unsmoothed WET (cm)
@@ -213,8 +214,11 @@ void *mapped_host_range(const void *host, size_t bytes);
 // is copied directly.  A pageable one is pipelined through the context's
 // pinned slabs: host threads copy slab c into a pinned buffer while the DMA
 // of slab c-1 runs, instead of the driver staging the whole volume serially.
+// With `on_slab`, the copy goes in slabs either way and on_slab(z) is called
+// after each slab's copy is enqueued, z = the planes enqueued so far, so that
+// the caller can enqueue work on those planes behind it.
 void upload_host_volume(DeviceContext &ctx, const float *src, int nz, int ny, int nx, VolumeArray *arr, float *lin,
-                        cudaStream_t s);
+                        cudaStream_t s, const std::function<void(int)> &on_slab = nullptr);
 
 // Throws Error(DC_ERR_CUDA) if the last launch failed.
 void check_launch(const char *kernel);
