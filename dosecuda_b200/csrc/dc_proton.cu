@@ -687,12 +687,12 @@ __device__ __forceinline__ void pb_tile(const Grid &g, const Frame &f, const Pro
 
 
 // Minimum resident CTAs per SM the register allocation is held to: 4 CTAs
-// of 256 threads (64 registers) for the one-shot kernel, 3 of 256 (or 6 of
-// 128) for the persistent batch kernel.  More resident warps hide the
-// fixed-latency chains of the spot loop and the per-layer barriers; measured
-// on the adjoint (0.492 -> 0.439 ms) and the batch (41.4 -> 35.2 ms for four
-// plans) with the dose kernel unchanged, despite a few spilled words outside
-// the spot loop.
+// of 256 threads (or 8 of 128; 64 registers) for the one-shot and the
+// persistent batch kernels.  More resident warps hide the fixed-latency
+// chains of the spot loop and the per-layer barriers; measured on the adjoint
+// (0.492 -> 0.439 ms) and the batch (41.4 -> 35.2 ms for four plans at 3 CTAs
+// of 256 threads, 16.7 -> 15.2 ms at 4 with the 16 x TY x 8 tiles) with the
+// dose kernel unchanged, despite a few spilled words outside the spot loop.
 constexpr int pb_min_ctas(int ty, int per_256) { return ty >= 8 ? per_256 : 2 * per_256; }
 
 // One tile per CTA (grid = the tiles of the volume, pb_tiles).
@@ -737,19 +737,37 @@ __global__ void __launch_bounds__(kPbThreadsX *TY, pb_min_ctas(TY, 4))
 // Persistent batch kernel: CTAs take (plan, tile) work items from a device
 // queue (most expensive plans first) and sum the dose of all the plan's beams
 // for the tile in registers before one write per voxel.
+//
+// The plan and beam records are staged in shared memory and passed to pb_tile
+// by reference: their fields are then read from shared memory where used
+// instead of holding some twenty registers through the layer loop (the
+// one-beam kernels read the same fields from the kernel parameters).
+template <class T>
+__device__ __forceinline__ void pb_stage_record(T *dst, const T *__restrict__ src, int tid, int nthreads) {
+    static_assert(sizeof(T) % sizeof(int) == 0, "records are copied as words");
+    const int *s = reinterpret_cast<const int *>(src);
+    int *d = reinterpret_cast<int *>(dst);
+    for (int q = tid; q < (int)(sizeof(T) / sizeof(int)); q += nthreads) d[q] = __ldg(s + q);
+}
+
 template <int TY, int VY>
-__global__ void __launch_bounds__(kPbThreadsX *TY, pb_min_ctas(TY, 3))
+__global__ void __launch_bounds__(kPbThreadsX *TY, pb_min_ctas(TY, 4))
     pb_batch_kernel(const PbBatchPlan *__restrict__ plans, const PbBatchBeam *__restrict__ beams,
                     const int2 *__restrict__ items, int n_items, unsigned *__restrict__ next) {
     __shared__ int s_item;
+    __shared__ PbBatchPlan s_plan;
+    __shared__ PbBatchBeam s_beam;
+    const int tid = threadIdx.y * kPbThreadsX + threadIdx.x;
     while (true) {
-        __syncthreads();
-        if (threadIdx.x == 0 && threadIdx.y == 0) s_item = (int)atomicAdd(next, 1u);
+        __syncthreads();  // the previous item's plan record no longer in use
+        if (tid == 0) s_item = (int)atomicAdd(next, 1u);
         __syncthreads();
         const int it = s_item;
         if (it >= n_items) break;
         const int2 w = items[it];
-        const PbBatchPlan P = plans[w.x];
+        pb_stage_record(&s_plan, plans + w.x, tid, kPbThreadsX * TY);
+        __syncthreads();
+        const PbBatchPlan &P = s_plan;
         const int3 nt = pb_tiles<TY, VY>(P.g);
         const int bz = w.y / (nt.x * nt.y);
         const int rem = w.y - bz * nt.x * nt.y;
@@ -757,11 +775,14 @@ __global__ void __launch_bounds__(kPbThreadsX *TY, pb_min_ctas(TY, 3))
         float acc[VY];
 #pragma unroll
         for (int v = 0; v < VY; ++v) acc[v] = 0.0f;
-        for (int b = P.beam0; b < P.beam0 + P.n_beams; ++b) {
-            const PbBatchBeam B = beams[b];
+        const int b1 = P.beam0 + P.n_beams;
+        for (int b = P.beam0; b < b1; ++b) {
+            __syncthreads();  // the previous beam's record no longer in use
+            pb_stage_record(&s_beam, beams + b, tid, kPbThreadsX * TY);
+            __syncthreads();
             PbExtra x;
-            x.mu = B.mu;
-            pb_tile<kPbDose, TY, VY>(P.g, B.f, B.t, B.wet, bx, by, bz, acc, x);
+            x.mu = s_beam.mu;
+            pb_tile<kPbDose, TY, VY>(P.g, s_beam.f, s_beam.t, s_beam.wet, bx, by, bz, acc, x);
         }
 #pragma unroll
         for (int v = 0; v < VY; ++v) {
