@@ -86,6 +86,7 @@ SIGNATURES = {
     "dc_release_device": (C.c_int, [C.c_int]),
     "dc_photon_set_depth_mode": (C.c_int, [C.c_int, C.c_int]),
     "dc_photon_get_depth_mode": (C.c_int, [C.c_int, C.POINTER(C.c_int)]),
+    "dc_photon_head_selftest": (C.c_int, [C.c_int, C.POINTER(C.c_float), C.POINTER(C.c_float)]),
     "dc_photon_depth_stats": (C.c_int, [C.c_int, C.POINTER(C.c_longlong)]),
     "dc_profile_enable": (C.c_int, [C.c_int, C.c_int]),
     "dc_profile_reset": (C.c_int, [C.c_int]),

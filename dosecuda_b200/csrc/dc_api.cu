@@ -198,6 +198,16 @@ int dc_photon_depth_stats(int gpu_id, long long *marched) {
     });
 }
 
+int dc_photon_head_selftest(int gpu_id, float *largest_unsaturated, float *skip_bound) {
+    return guarded([&] {
+        need(largest_unsaturated != nullptr && skip_bound != nullptr, "output pointers must not be NULL.");
+        DeviceContext &ctx = context(gpu_id);
+        std::lock_guard<std::mutex> lk(ctx.mu);
+        *largest_unsaturated = photon_erf_unsaturated(3.0f, 4.5f);
+        *skip_bound = photon_erf_skip_bound();
+    });
+}
+
 int dc_profile_enable(int gpu_id, int on) {
     return guarded([&] {
         DeviceContext &ctx = context(gpu_id);

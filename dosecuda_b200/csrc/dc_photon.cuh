@@ -64,6 +64,11 @@ struct PhotonWork {
 // transmission, off-axis factors) on the context's side stream, after the
 // work enqueued on s so far.  The next enqueue_terma joins it; without this
 // call enqueue_terma forks it itself, beside the depth pass.
+// Head-transmission skip bound check: the largest float x in [lo, hi] whose
+// device erff(+-x) is not exactly +-1 (0 when there is none; synchronous,
+// current device), and the bound the head kernel skips leaf pairs beyond.
+float photon_erf_unsaturated(float lo, float hi);
+float photon_erf_skip_bound();
 void photon_head_fork(DeviceContext &ctx, const Grid &g, const Frame &f, const PhotonParams &P, cudaStream_t s);
 // Ray trace + TERMA + cone directions.  dose_dev (or null) receives the zero
 // of every masked voxel, terma_out (or null) a linear TERMA copy.

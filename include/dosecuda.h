@@ -176,6 +176,14 @@ int dc_photon_get_depth_mode(int gpu_id, int *mode);
  * exactly (its fallback); -1 when the last pass marched every voxel or none
  * ran.  Synchronises the device. */
 int dc_photon_depth_stats(int gpu_id, long long *marched);
+/* Self-test of the head transmission's leaf-pair skip (replaces nothing in
+ * the reference, which evaluates every pair, headTransmission
+ * IMRTClasses.cu:120-150): *largest_unsaturated = the largest float x in
+ * [3, 4.5] for which the device's erff(x) != 1 or erff(-x) != -1 (0 if
+ * none), *skip_bound = the edge argument beyond which the kernel skips a
+ * pair.  The skip leaves every sum bitwise unchanged when
+ * largest_unsaturated <= skip_bound.  Synchronous. */
+int dc_photon_head_selftest(int gpu_id, float *largest_unsaturated, float *skip_bound);
 
 /* Kernel timing: when enabled, every kernel the library launches is
  * bracketed by CUDA events on its own stream.  dc_profile_read synchronises
